@@ -1,0 +1,138 @@
+"""ctypes binding of libbeamz_b200.so (declarations: include/beamz_b200.h).
+
+The shared library is the only compute path: importing this module fails with
+an ImportError naming the missing file when the library has not been built, and
+every entry raises ``RuntimeError`` with the library's message on a non-zero
+status. There is no fallback implementation.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from pathlib import Path
+
+_LIB_PATH = Path(os.environ.get("BEAMZ_B200_LIB", Path(__file__).resolve().parent / "libbeamz_b200.so"))
+
+if not _LIB_PATH.exists():
+    raise ImportError(
+        f"libbeamz_b200.so not found at {_LIB_PATH}; build it with `python -m beamz_b200._build` "
+        "(needs nvcc for sm_100a)"
+    )
+
+try:
+    lib = C.CDLL(str(_LIB_PATH))
+except OSError as exc:  # e.g. libcudart missing on a machine without CUDA
+    raise ImportError(f"cannot load {_LIB_PATH}: {exc}") from exc
+
+BZ_OK = 0
+BZ_ERR_INVALID = -1
+BZ_ERR_CUDA = -2
+BZ_ERR_DIVERGED = -3
+BZ_ERR_TIMEOUT = -4
+BZ_ERR_UNSUPPORTED = -5
+BZ_F32 = 0
+BZ_F64 = 1
+BZ_SHAPE_RECT, BZ_SHAPE_CIRCLE, BZ_SHAPE_RING, BZ_SHAPE_POLYGON = 0, 1, 2, 3
+
+i32, i64, f64, vp = C.c_int32, C.c_int64, C.c_double, C.c_void_p
+
+
+class Grid2D(C.Structure):
+    _fields_ = [("nx", i32), ("ny", i32), ("pitch", i32), ("n_designs", i32), ("n_comp", i32), ("n_mat", i32),
+                ("dtype", i32), ("reserved", i32), ("chx", f64), ("chy", f64), ("qy", f64), ("inv_kd2", f64)]
+
+
+class Fields2D(C.Structure):
+    _fields_ = [("ez", vp * 2), ("hx", vp * 2), ("hy", vp * 2), ("ce", vp), ("loss", vp), ("power", vp)]
+
+
+class SourceOps(C.Structure):
+    _fields_ = [("n_ops", i32), ("n_steps", i32), ("row_ptr", vp), ("cell", vp), ("mul", vp), ("weight", vp),
+                ("sig", vp), ("signals", vp)]
+
+
+class MonitorOps(C.Structure):
+    _fields_ = [("n_points", i32), ("n_freq", i32), ("row_ptr", vp), ("cell", vp), ("point", vp), ("record", vp),
+                ("rec_step0", i64), ("n_rec", i32), ("n_phasor", i32), ("dft", vp), ("phasor", vp)]
+
+
+class Shape2D(C.Structure):
+    _fields_ = [("kind", i32), ("i0", i32), ("i1", i32), ("j0", i32), ("j1", i32), ("fill", i32), ("fi0", i32),
+                ("fi1", i32), ("fj0", i32), ("fj1", i32), ("top", i32), ("bottom", i32), ("left", i32),
+                ("right", i32), ("path0", i32), ("npath", i32), ("custom_off", i32), ("reserved", i32),
+                ("p0", f64), ("p1", f64), ("p2", f64), ("p3", f64), ("q", f64), ("perm", f64), ("permb", f64),
+                ("cond", f64)]
+
+
+class Pml2D(C.Structure):
+    _fields_ = [("i0", i32), ("i1", i32), ("j0", i32), ("j1", i32), ("table_off", i64), ("sigma_factor", f64)]
+
+
+def _sig(name, restype, argtypes):
+    fn = getattr(lib, name)
+    fn.restype = restype
+    fn.argtypes = argtypes
+    return fn
+
+
+_version = _sig("bz_version", C.c_char_p, [])
+_last_error = _sig("bz_last_error", C.c_int, [C.c_char_p, C.c_size_t])
+_step2d = _sig("bz_step2d", C.c_int, [C.POINTER(Grid2D), C.POINTER(Fields2D), C.POINTER(SourceOps),
+                                       C.POINTER(MonitorOps), i64, vp, vp])
+_advance = _sig("bz_advance_step", C.c_int, [vp, i64, vp])
+_prepare = _sig("bz_prepare_coeffs", C.c_int, [vp, vp, i64, i32, i32, i32, f64, f64, f64, vp, vp, vp])
+_upd_h2d = _sig("bz_update_h2d", C.c_int, [i32, i32, i32, i32, vp, vp, vp, vp, f64, f64, f64, f64, f64, vp])
+_upd_e2d = _sig("bz_update_e2d", C.c_int, [i32, i32, i32, i32, vp, vp, vp, vp, vp, f64, f64, f64, f64, vp])
+_raster2d = _sig("bz_rasterize2d", C.c_int, [i32, i32, vp, vp, vp, vp, vp, vp, i32, vp, vp, vp, vp, i32, vp,
+                                              f64, f64, f64, vp, vp, vp, vp])
+
+#: every symbol include/beamz_b200.h declares (checked by the CPU test suite)
+EXPORTED = ["bz_version", "bz_last_error", "bz_step2d", "bz_advance_step", "bz_prepare_coeffs", "bz_update_h2d",
+            "bz_update_e2d", "bz_rasterize2d"]
+
+
+class NativeError(RuntimeError):
+    def __init__(self, code: int, message: str):
+        super().__init__(f"libbeamz_b200 error {code}: {message}")
+        self.code = code
+
+
+def last_error() -> tuple[int, str]:
+    buf = C.create_string_buffer(512)
+    code = _last_error(buf, len(buf))
+    return code, buf.value.decode(errors="replace")
+
+
+def check(status: int) -> None:
+    if status != BZ_OK:
+        code, msg = last_error()
+        raise NativeError(status, msg or f"status {status}")
+
+
+def version() -> str:
+    return _version().decode()
+
+
+def step2d(grid, fields, src, mon, step: int, d_step: int | None, stream: int) -> None:
+    check(_step2d(C.byref(grid), C.byref(fields), C.byref(src) if src is not None else None,
+                  C.byref(mon) if mon is not None else None, step, d_step, stream))
+
+
+def advance_step(d_step: int, n: int, stream: int) -> None:
+    check(_advance(d_step, n, stream))
+
+
+def prepare_coeffs(eps, sigma, rows, nx, pitch, dtype, dt, eps0, dy, ce, loss, stream) -> None:
+    check(_prepare(eps, sigma, rows, nx, pitch, dtype, dt, eps0, dy, ce, loss, stream))
+
+
+def rasterize2d(*args) -> None:
+    check(_raster2d(*args))
+
+
+def update_h2d(*args) -> None:
+    check(_upd_h2d(*args))
+
+
+def update_e2d(*args) -> None:
+    check(_upd_e2d(*args))

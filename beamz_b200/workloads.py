@@ -1,0 +1,90 @@
+"""Synthetic benchmark workloads: the design, time axis, sources and monitors of
+the standard configurations, built through the public API.
+
+* ``dipole_2d``  400x400 cells at 20 nm, vacuum, 20-cell order-3 PML, point-like
+  Gaussian source with a Gaussian-pulsed carrier at 1.55 um, 2000 steps, four edge
+  line monitors.
+* ``mmi_2d``     2000x1000 cells at 20 nm, SiO2 cladding (eps 2.085) with a Si
+  (eps 12.25) 1x2 MMI: 500 nm input/output guides, 6 x 3 um body, outputs at
+  +-0.75 um; 30-cell PML; CW (ramped cosine) fundamental-mode source at 1.55 um;
+  20000 steps; DFT flux monitors at 1.50..1.60 um on the input and both ports.
+
+PML grading: order 3 with sigma_max set for a normal-incidence reflection R = 1e-6,
+sigma_max = (m+1) ln(1/R) / (2 eta0 d), d = thickness; expressed through the
+PML's ``sigma_factor`` relative to its default 1.2/(eta0 dx).
+"""
+from __future__ import annotations
+
+import numpy as np
+
+from .const import LIGHT_SPEED, µm
+from .design.core import Design
+from .design.materials import Material
+from .design.structures import Rectangle
+from .devices.monitors import Monitor
+from .devices.signals import gaussian_pulse, ramped_cosine
+from .devices.sources import GaussianSource, ModeSource
+
+
+def pml_sigma_factor(n_cells: int, order: int = 3, reflection: float = 1e-6) -> float:
+    """sigma_factor giving sigma_max = (m+1) ln(1/R) / (2 eta0 n dx) (eta0 cancels)."""
+    return (order + 1) * np.log(1.0 / reflection) / (2.0 * n_cells) / 1.2
+
+
+def _grade(design, n_cells):
+    for b in design.boundaries:
+        b.polynomial_order = 3
+        b.sigma_factor = pml_sigma_factor(n_cells)
+    return design
+
+
+def courant_dt(dx, dims=2):
+    return 0.99 * dx / (LIGHT_SPEED * np.sqrt(dims))
+
+
+def dipole_2d(n=400, dx=0.02 * µm, n_steps=2000, pml=20):
+    W = (n + 0.5) * dx
+    d = _grade(Design(width=W, height=W, material=Material(1.0), pml_size=pml * dx), pml)
+    t = np.arange(n_steps) * courant_dt(dx)
+    sig = gaussian_pulse(t, 1.0, 3 * 10e-15, 10e-15, LIGHT_SPEED / (1.55 * µm), 0.0)
+    d += GaussianSource(position=(n // 2 * dx, n // 2 * dx), width=dx / 10, signal=sig)
+    k = (pml + 10) * dx
+    lo, hi = k, (n - pml - 10) * dx
+    mons = [Monitor(design=d, start=(lo, lo), end=(lo, hi), name="left"),
+            Monitor(design=d, start=(hi, lo), end=(hi, hi), name="right"),
+            Monitor(design=d, start=(lo, lo), end=(hi, lo), name="bottom"),
+            Monitor(design=d, start=(lo, hi), end=(hi, hi), name="top")]
+    for m in mons:
+        d += m
+    return d, t, dx
+
+
+MMI_WAVELENGTHS = np.array([1.50, 1.525, 1.55, 1.575, 1.60]) * µm
+
+
+def mmi_2d(nx=2000, ny=1000, dx=0.02 * µm, n_steps=20000, pml=30, mode_solver="num_eigen"):
+    W, H = (nx + 0.5) * dx, (ny + 0.5) * dx
+    d = _grade(Design(width=W, height=H, material=Material(2.085), pml_size=pml * dx), pml)
+    yc, xc = H / 2, W / 2
+    si = Material(12.25)
+    wg, L, B, off = 0.5 * µm, 6.0 * µm, 3.0 * µm, 0.75 * µm
+    d += Rectangle(position=(0, yc - wg / 2), width=xc - L / 2, height=wg, material=si)
+    d += Rectangle(position=(xc - L / 2, yc - B / 2), width=L, height=B, material=si)
+    for s in (+1, -1):
+        d += Rectangle(position=(xc + L / 2, yc + s * off - wg / 2), width=W - (xc + L / 2), height=wg, material=si)
+    t = np.arange(n_steps) * courant_dt(dx)
+    sig = ramped_cosine(t, amplitude=1.0, frequency=LIGHT_SPEED / (1.55 * µm), phase=0,
+                        ramp_duration=20 * 1.55 * µm / LIGHT_SPEED, t_max=t[-1] * 2)
+    x_src = pml * dx + 1.0 * µm
+    d += ModeSource(design=d, position=(x_src, yc), width=2.0 * µm, wavelength=1.55 * µm, signal=sig, direction="+x",
+                    num_modes=1, mode_solver=mode_solver)
+    x_in, x_out = x_src + 1.0 * µm, W - pml * dx - 1.0 * µm
+    mons = [Monitor(design=d, start=(x_in, yc - 1.0 * µm), end=(x_in, yc + 1.0 * µm), name="in",
+                    wavelengths=MMI_WAVELENGTHS, record_fields=False, accumulate_power=False)]
+    for s, name in ((+1, "port_top"), (-1, "port_bottom")):
+        y0 = yc + s * off
+        mons.append(Monitor(design=d, start=(x_out, y0 - 0.6 * µm), end=(x_out, y0 + 0.6 * µm), name=name,
+                            wavelengths=MMI_WAVELENGTHS, record_fields=False, accumulate_power=False))
+    for m in mons:
+        d += m
+    return d, t, dx

@@ -1,0 +1,340 @@
+#!/usr/bin/env python
+"""Benchmark of the FDTD stepping path: Gcell-updates/s on the 2D MMI workload.
+
+Workload (default ``mmi_2d``): 2000 x 1000 cells at 20 nm, Si 1x2 MMI in SiO2,
+30-cell order-3 PML, CW mode source, DFT flux monitors at 5 wavelengths on the
+input and both output ports, 20000 time steps. One bench step = one full run of
+all 20000 time steps from zero fields. The grid (fields + coefficients, 64 MB)
+fits in L2, so L2 is flushed (a 512 MB write) before every run.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+Prints one JSON line (rank 0). With N > 1 (torchrun) every rank runs its own
+replica of the workload ("replicas only": the path has no exchange step); value
+is the total cell updates of all ranks over the slowest rank's time.
+
+``--impl reference`` times the reference algorithm's CPU implementation (the
+float64 NumPy restatement in oracle/, operation-for-operation the reference's
+NumPy backend and step helpers) on a bounded sample of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "Gcell-updates/s (% of HBM roofline)"
+UNIT = "Gcell/s"
+BYTES_PER_CELL_2D = 32  # Ez, Hx, Hy read + write (24 B) + ce, loss (8 B), float32
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=5)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    p.add_argument("--workload", default="mmi_2d", choices=["mmi_2d", "dipole_2d"])
+    p.add_argument("--time-steps", type=int, default=None, help="override the workload's step count")
+    p.add_argument("--cpu-steps", type=int, default=60, help="time steps of the CPU baseline sample")
+    p.add_argument("--no-e2e", action="store_true")
+    return p.parse_args()
+
+
+def workload(name, n_steps=None):
+    from beamz_b200 import workloads as W
+
+    kw = {} if n_steps is None else {"n_steps": n_steps}
+    d, t, dx = getattr(W, name)(**kw)
+    desc = {"mmi_2d": "2D TE 1x2 MMI splitter, 2000x1000 cells at 20 nm, 30-cell PML, CW mode source, "
+                      "5-wavelength DFT flux monitors",
+            "dipole_2d": "2D point dipole in vacuum, 400x400 cells at 20 nm, 20-cell PML, 4 edge monitors"}[name]
+    return d, t, dx, desc
+
+
+# ---------------------------------------------------------------------------- clocks
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_id: str):
+        self.gpu_id = gpu_id
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                          "-lms", "200", "-i", self.gpu_id], stdout=open(self.path, "w"),
+                                         stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        rows = [r.split(",") for r in Path(self.path).read_text().splitlines() if r.strip()]
+        os.unlink(self.path)
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            try:
+                sm.append(float(r[1]))
+                mx = float(r[2])
+            except (ValueError, IndexError):
+                continue
+            for nm, v in zip(names, r[5:9]):
+                if v.strip().lower() in ("active", "1"):
+                    reasons.add(nm)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------- helpers
+def measured_peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def profiled_traffic(kernel="step2d", workload_name="mmi_2d"):
+    """dram bytes per launch from the committed ncu summary, if present."""
+    p = ROOT / "profiles" / f"{kernel}_{workload_name}.txt"
+    if not p.exists():
+        return None
+    for line in p.read_text().splitlines():
+        if line.startswith("traffic_bytes_per_launch:"):
+            try:
+                return float(line.split(":", 1)[1])
+            except ValueError:
+                return None
+    return None
+
+
+def cpu_baseline(d, t, dx, n_steps):
+    """The reference's CPU loop (oracle restatement) on the first n_steps of the workload."""
+    from beamz_b200.simulation.meshing import RegularGrid  # noqa: F401 - grid from the caller
+    from oracle import fdtd2d
+
+    eps, sig = d._bench_eps, d._bench_sigma
+    mons = [m for m in d.monitors]
+    t0 = time.perf_counter()
+    fdtd2d.run(eps, sig, dx, dx, t[1] - t[0], n_steps, d.sources, mons, record=True)
+    el = time.perf_counter() - t0
+    cells = eps.size
+    return cells * n_steps / el / 1e9, el
+
+
+# ---------------------------------------------------------------------------- b200 arm
+def run_b200(args):
+    import torch
+    import torch.distributed as dist
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    from beamz_b200 import FDTD, RegularGrid
+
+    d, t, dx, desc = workload(args.workload, args.time_steps)
+    grid = RegularGrid(d, dx)
+    ny, nx = grid.permittivity.shape
+    cells = nx * ny
+    n_steps = len(t)
+    sim = FDTD(design=grid, time=t)
+    sim.initialize_simulation(save=False, live=False, save_memory_mode=True)
+    eng = sim.engine
+    flush = torch.empty(512 << 20, dtype=torch.uint8, device="cuda")
+
+    def reset():
+        for bufs in (eng.ez, eng.hx, eng.hy):
+            for b in bufs:
+                b.zero_()
+        if eng.dft is not None:
+            eng.dft.zero_()
+        eng.step_index = 0
+
+    def one_run(evs=None):
+        reset()
+        flush.fill_(1)
+        if evs is not None:
+            evs[0].record()
+        eng.run_steps(n_steps)
+        if evs is not None:
+            evs[1].record()
+
+    for _ in range(args.warmup):
+        one_run()
+    torch.cuda.synchronize()
+    gpu_id = "GPU-" + str(torch.cuda.get_device_properties(local).uuid)
+    clocks = ClockSampler(gpu_id)
+    clocks.start()
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    t_start = torch.cuda.Event(enable_timing=True)
+    t_end = torch.cuda.Event(enable_timing=True)
+    t_start.record()
+    for k in range(args.steps):
+        one_run(evs[k])
+    t_end.record()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    ck = clocks.stop()
+    total_ms = t_start.elapsed_time(t_end)
+    run_ms = [a.elapsed_time(b) for a, b in evs]
+    if world > 1:
+        tt = torch.tensor([total_ms], device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        total_ms = float(tt.item())
+    value = world * args.steps * cells * n_steps / (total_ms * 1e-3) / 1e9
+
+    # dominant kernel: the fused step launch (one per time step)
+    per_launch_s = sum(run_ms) * 1e-3 / (args.steps * n_steps)
+    algo_bytes = BYTES_PER_CELL_2D * cells
+    peak, peak_kind = measured_peaks()
+    achieved = algo_bytes / per_launch_s / 1e9
+    traffic = profiled_traffic("step2d", args.workload)
+
+    e2e = None
+    if not args.no_e2e:
+        e2e = run_e2e(grid, t, cells, n_steps, args, world)
+
+    cpu = None
+    if rank == 0 and world == 1:
+        d._bench_eps, d._bench_sigma = grid.permittivity, grid.conductivity
+        ncpu = min(args.cpu_steps, n_steps)
+        v, el = cpu_baseline(d, t, dx, ncpu)
+        cpu = {"value": v, "unit": UNIT, "cores": 1, "kind": "port",
+               "sample": f"first {ncpu} of {n_steps} time steps of the same workload, float64 NumPy "
+                         f"(the reference's NumPy backend and step helpers restated in oracle/), {el:.1f} s"}
+    flux = None
+    try:
+        sim2 = e2e.pop("_sim") if e2e else None
+        if sim2 is not None:
+            tin = next(m for m in sim2.monitors if m.name == "in").flux()
+            tp = [next(m for m in sim2.monitors if m.name == n).flux() for n in ("port_top", "port_bottom")]
+            flux = {"T_top": list(np.round(tp[0] / tin, 4)), "T_bottom": list(np.round(tp[1] / tin, 4))}
+    except Exception:  # noqa: BLE001 - the transmission readout is informational only
+        flux = None
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(total_ms / args.steps, 3), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": desc, "grid": [ny, nx], "time_steps": n_steps, "step": "one full run",
+                       "l2": "flushed (512 MB write) before every run", "parallelism": f"replicas x{world}"},
+            "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                         "frac": round(achieved / peak, 4), "traffic": traffic,
+                         "note": f"step2d algorithmic bytes {BYTES_PER_CELL_2D} B/cell x {cells} cells per launch; "
+                                 f"peak {peak_kind}; grid is L2-resident within a run"},
+            "cpu_baseline": cpu,
+            "e2e": {k: v for k, v in (e2e or {}).items() if not k.startswith("_")} or None,
+            "gpu_launches": args.steps * n_steps,
+            "clocks": ck,
+        }
+        if flux:
+            line["transmission"] = flux
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def run_e2e(grid, t, cells, n_steps, args, world):
+    """Same metric through the public API: FDTD(design=grid).run() from host arrays,
+    H2D of material/sources/monitor tables and D2H of the DFT results inside."""
+    import torch
+
+    from beamz_b200 import FDTD
+
+    times = []
+    sim = None
+    h2d = d2h = 0
+    for k in range(max(1, min(args.steps, 3))):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        sim = FDTD(design=grid, time=t)
+        sim.run(live=False, save=False, save_memory_mode=True)
+        torch.cuda.synchronize()
+        times.append(time.perf_counter() - t0)
+        eng = sim.engine
+        h2d = eng.h2d_bytes
+        d2h = eng.d2h_bytes
+    el = float(np.median(times))
+    return {"value": round(world * cells * n_steps / el / 1e9, 3), "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+            "d2h_bytes_per_step": int(d2h), "seconds_per_run": round(el, 4), "_sim": sim}
+
+
+# ---------------------------------------------------------------------------- reference arm
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    d, t, dx, desc = workload(args.workload, args.time_steps)
+    from beamz_b200.devices.sources import GaussianSource  # noqa: F401
+    from oracle import fdtd2d
+
+    eps, sig = _host_grid(d, dx)
+    sample = max(1, min(20, len(t)))
+    cells = eps.size
+    for _ in range(args.warmup):
+        fdtd2d.run(eps, sig, dx, dx, t[1] - t[0], sample, d.sources, d.monitors, record=True)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        fdtd2d.run(eps, sig, dx, dx, t[1] - t[0], sample, d.sources, d.monitors, record=True)
+    el = time.perf_counter() - t0
+    value = args.steps * cells * sample / el / 1e9
+    line = {"impl": "reference", "metric": METRIC, "value": round(value, 5), "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(el / args.steps * 1e3, 3),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": desc, "grid": list(eps.shape), "time_steps_per_step": sample,
+                       "parallelism": "1 host core (NumPy elementwise)"},
+            "cpu_baseline": {"value": round(value, 5), "unit": UNIT, "cores": 1, "kind": "port",
+                             "sample": f"{sample} time steps of the workload per bench step, float64 NumPy"},
+            "e2e": {"value": round(value, 5), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def _host_grid(d, dx):
+    """Material arrays for the CPU arm from the oracle's host rasteriser (the
+    reference's meshing restated; bit-identical to the GPU rasteriser's output)."""
+    from oracle import raster2d
+
+    return raster2d.rasterize(d, dx)
+
+
+if __name__ == "__main__":
+    a = parse()
+    if a.impl == "reference":
+        run_reference(a)
+    else:
+        run_b200(a)

@@ -1,0 +1,218 @@
+/*
+ * beamz_b200 — C ABI of the B200-native FDTD stepping library (libbeamz_b200.so).
+ *
+ * Conventions
+ *   - Plain C types only: pointers are device pointers unless stated otherwise,
+ *     sizes are element counts. No C++ exceptions cross this boundary.
+ *   - Every entry returns an int status: BZ_OK (0) or a negative BZ_ERR_* code.
+ *     bz_last_error() copies the message of the last failure on this thread.
+ *   - The library allocates no device memory. Callers own every buffer.
+ *   - Streams are passed as void* (a cudaStream_t); NULL is the legacy stream.
+ *   - Layouts: 2D arrays are row-major [y][x] with x contiguous and a row pitch
+ *     (elements) that is a multiple of 32; a batch of fields is laid out as
+ *     [design][component][ny][pitch]. 3D arrays are [z][y][x], x contiguous,
+ *     with the same padded pitch and a plane stride of ny*pitch.
+ *   - dtype codes: BZ_F32 (0) or BZ_F64 (1) for field and coefficient arrays.
+ *
+ * Reference interfaces replaced (paths inside the beamz project):
+ *   bz_step2d       beamz/simulation/backends/numpy_backend.py:34-88
+ *                   (update_h_fields + update_e_field), beamz/simulation/helper.py:5-118
+ *                   (apply_sources), helper.py:120-187 (accumulate_power),
+ *                   helper.py:231-256 + beamz/devices/monitors.py:279-315 (record_monitor_data)
+ *   bz_step3d       beamz/simulation/fdtd.py:200-310 (_update_3d_fields) + the same helpers
+ *   bz_prepare_coeffs  the per-step coefficient arithmetic of numpy_backend.py:52-60,80-84
+ *                   and fdtd.py:232-305, hoisted out of the time loop
+ *   bz_rasterize2d  beamz/simulation/meshing.py:92-536 (RegularGrid.__rasterize__)
+ *   bz_rasterize3d  beamz/simulation/meshing.py:616-781 (RegularGrid3D.__rasterize_3d__)
+ */
+#ifndef BEAMZ_B200_H
+#define BEAMZ_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define BZ_OK 0
+#define BZ_ERR_INVALID (-1)     /* bad argument: null pointer, shape, stride, dtype */
+#define BZ_ERR_CUDA (-2)        /* a CUDA runtime call failed */
+#define BZ_ERR_DIVERGED (-3)    /* non-finite or runaway field detected */
+#define BZ_ERR_TIMEOUT (-4)     /* a bounded device wait ran out */
+#define BZ_ERR_UNSUPPORTED (-5) /* valid request that this build does not handle */
+
+#define BZ_F32 0
+#define BZ_F64 1
+
+/* Library version string, e.g. "beamz_b200 0.1.0 sm_100a". Never fails. */
+const char* bz_version(void);
+
+/* Copies the last error message of the calling thread into buf (NUL-terminated,
+ * truncated to len). Returns the status code of that error (BZ_OK if none). */
+int bz_last_error(char* buf, size_t len);
+
+/* ----------------------------------------------------------------------------
+ * Grid description shared by the 2D entries.
+ *   nx, ny        cells of the permittivity grid (RegularGrid.permittivity.shape = (ny, nx))
+ *   pitch         row pitch in elements (>= nx, multiple of 32)
+ *   n_designs     independent designs stepped in one launch
+ *   n_comp        field components per design: 1 = real field, 2 = (Re, Im)
+ *   n_mat         coefficient sets: 1 (shared by all designs) or n_designs
+ *   dtype         BZ_F32 / BZ_F64 for fields and coefficients
+ *   chx, chy      dt/(mu0*dy) and dt/(mu0*dx): H-update factors for x- and y-differences
+ *                 (the reference divides x-differences by dy and y-differences by dx,
+ *                  numpy_backend.py:47-48; the same pairing is kept)
+ *   qy            dy/dx: weight of the y-difference in the E curl relative to the x one
+ *   inv_kd2       2*eps0*dy/dt: converts (loss * ce) into the E loss factor
+ * -------------------------------------------------------------------------- */
+typedef struct bz_grid2d {
+  int32_t nx, ny, pitch;
+  int32_t n_designs, n_comp, n_mat;
+  int32_t dtype;
+  int32_t reserved;
+  double chx, chy, qy, inv_kd2;
+} bz_grid2d;
+
+/* Field and coefficient buffers of one 2D problem. ez/hx/hy hold two ping-pong
+ * copies each; a launch with host-side step argument n reads copy (n & 1) and
+ * writes copy (n & 1) ^ 1.
+ * ce   = dt/(eps0*dy*(eps_r + a))   (E update source factor, x-difference units)
+ * loss = a = sigma*dt/(2*eps0)      (dimensionless conductivity term)
+ * power (optional, float64 [n_designs][ny][pitch]) accumulates |S|^2 per cell as
+ * helper.py:153-187 does. */
+typedef struct bz_fields2d {
+  void* ez[2];
+  void* hx[2];
+  void* hy[2];
+  const void* ce;
+  const void* loss;
+  double* power;
+} bz_fields2d;
+
+/* Source injection after the E update (helper.py:5-118), as a list of cell
+ * operations applied in list order: v = mul*v + sum_c weight*signal[sig][step].
+ * cell is the linear index y*nx + x (3D: (z*ny + y)*nx + x), sorted ascending with
+ * operations on the same cell kept in application order. */
+typedef struct bz_source_ops {
+  int32_t n_ops;
+  int32_t n_steps;          /* length of each signal row; later steps inject nothing */
+  const int32_t* row_ptr;   /* [rows+1]: ops of grid row r (2D: y, 3D: z*ny+y) are [row_ptr[r], row_ptr[r+1]) */
+  const int32_t* cell;      /* [n_ops] */
+  const void* mul;          /* [n_ops] dtype: 1 keeps the old value, 0 zeroes it */
+  const void* weight;       /* [n_ops][n_comp] dtype */
+  const int32_t* sig;       /* [n_ops] signal row */
+  const void* signals;      /* [n_signals][n_steps] dtype */
+} bz_source_ops;
+
+/* Monitor sampling after injection (monitors.py:279-315). Each point samples,
+ * at its cell: Ez, Hx, Hy (the reference's record_fields_2d triple) and, for the
+ * DFT, the two neighbours used to centre H on the E node.
+ * record (optional): [n_rec][n_designs][n_comp][n_points][3] dtype, row
+ *   (step - rec_step0) for rec_step0 <= step < rec_step0 + n_rec.
+ * dft (optional, float64): [n_designs][n_comp][n_points][n_freq][5][2] running sums of
+ *   q * exp(-i w t) for q in (Ez, Hx(x), Hx(x-1), Hy(y), Hy(y-1)); phasor[step][f] =
+ *   (cos wtE, -sin wtE, cos wtH, -sin wtH) with tE = (step+1)dt, tH = (step+1/2)dt. */
+typedef struct bz_monitor_ops {
+  int32_t n_points;
+  int32_t n_freq;
+  const int32_t* row_ptr;   /* [rows+1] as in bz_source_ops */
+  const int32_t* cell;      /* [n_points] sorted ascending */
+  const int32_t* point;     /* [n_points] output slot of each sorted entry */
+  void* record;
+  int64_t rec_step0;
+  int32_t n_rec;
+  int32_t n_phasor;         /* rows of phasor; steps beyond it accumulate nothing */
+  double* dft;
+  const double* phasor;
+} bz_monitor_ops;
+
+/* One full time step of the 2D Ez-mode Yee scheme for every design and component:
+ * H update (all H cells), E update (interior, PEC ring), source injection,
+ * optional |S|^2 accumulation, monitor record + DFT.
+ * step: time-step index n; it also selects the ping-pong copy read (n & 1). If
+ * d_step is non-NULL the time index used for signals, records and DFT phasors is
+ * *d_step + step (CUDA-graph replay with a device-side step counter) while the
+ * copy read stays (step & 1). */
+int bz_step2d(const bz_grid2d* g, const bz_fields2d* f, const bz_source_ops* src,
+              const bz_monitor_ops* mon, int64_t step, const int64_t* d_step, void* stream);
+
+/* Adds n to the device step counter (*d_step += n). */
+int bz_advance_step(int64_t* d_step, int64_t n, void* stream);
+
+/* Coefficients from the rasterised material: float64 eps_r and sigma, dense
+ * [rows][nx] (rows = n*ny in 2D, n*nz*ny in 3D), into padded ce/loss arrays of
+ * dtype laid out [rows][pitch]; padding columns are written as 0.
+ *   ce   = dt/(eps0*dy*(eps_r + a)),  loss = a = sigma*dt/(2*eps0)
+ * This is the coefficient arithmetic of numpy_backend.py:52-60,80-84 and
+ * fdtd.py:232-305, evaluated once in float64 and rounded once to dtype. */
+int bz_prepare_coeffs(const double* eps_r, const double* sigma, int64_t rows, int32_t nx,
+                      int32_t pitch, int32_t dtype, double dt, double eps0, double dy,
+                      void* ce, void* loss, void* stream);
+
+/* Unfused half-step updates on arrays with the reference's shapes, for callers
+ * of the Backend interface (update_h_fields / update_e_field,
+ * beamz/simulation/backends/numpy_backend.py:34-88). Dense row-major arrays:
+ * Ez (ny, nx), Hx (ny, nx-1), Hy (ny-1, nx), sigma and eps_r (ny, nx), all of
+ * dtype; nc = 1 for real fields, 2 for interleaved (re, im) complex fields.
+ * H is updated everywhere, Ez in the interior only; both in place. */
+int bz_update_h2d(int32_t dtype, int32_t ny, int32_t nx, int32_t nc, void* hx, void* hy, const void* ez,
+                  const void* sigma, double dx, double dy, double dt, double mu0, double eps0, void* stream);
+int bz_update_e2d(int32_t dtype, int32_t ny, int32_t nx, int32_t nc, void* ez, const void* hx, const void* hy,
+                  const void* sigma, const void* eps_r, double dx, double dy, double dt, double eps0, void* stream);
+
+/* ----------------------------------------------------------------------------
+ * Rasteriser (meshing.py:92-536): painter's-order supersampled blend of each
+ * structure's material, then the additive PML conductivity pass.
+ * ------------------------------------------------------------------------- */
+#define BZ_SHAPE_RECT 0      /* axis-aligned rectangle fast path, meshing.py:193-257 */
+#define BZ_SHAPE_CIRCLE 1    /* circle fast path, meshing.py:259-307 */
+#define BZ_SHAPE_RING 2      /* ring fast path, meshing.py:309-361 */
+#define BZ_SHAPE_POLYGON 3   /* general polygon path, meshing.py:362-477 */
+
+typedef struct bz_shape2d {
+  int32_t kind;
+  int32_t i0, i1, j0, j1;        /* cell loop box [i0,i1) x [j0,j1) (rect: the rect box) */
+  int32_t fill;                  /* rect: interior fill applies */
+  int32_t fi0, fi1, fj0, fj1;    /* rect: interior fill box */
+  int32_t top, bottom, left, right; /* rect: boundary strips, rel row < top or >= bottom, rel col < left or >= right */
+  int32_t path0, npath;          /* polygon: rows of the path table (exterior first, then holes) */
+  int32_t custom_off;            /* rect with CustomMaterial: offset (in triples) into the custom table, else -1 */
+  int32_t reserved;
+  double p0, p1, p2, p3;         /* rect: x0, x0+w, y0, y0+h; circle: cx, cy, r; ring: cx, cy, rin, rout */
+  double q;                      /* circle/ring: 0.3536 * cell_size */
+  double perm, permb, cond;      /* material */
+} bz_shape2d;
+
+/* PML boundary (beamz/design/pml.py:29-62) over its loop box. table holds, for
+ * every cell of the box in row-major order, (profile, frequency_factor) or a
+ * negative profile where get_conductivity returns 0 — the position-only part,
+ * tabulated by the host. The kernel adds
+ *   ((1.2/(sqrt(mu0/(eps0*eps))*dx))*sigma_factor*profile)*frequency_factor
+ * when it is > 0. */
+typedef struct bz_pml2d {
+  int32_t i0, i1, j0, j1;
+  int64_t table_off;             /* offset (in pairs) into the pml table */
+  double sigma_factor;
+} bz_pml2d;
+
+/* eps/mu/sigma: float64 [ny][nx] outputs (fully written). xc[nx], yc[ny]: cell-centre
+ * coordinates (float64, the reference's np.linspace values). offs[3]: the
+ * supersample offsets (-0.25, 0, 0.25)*cell_size; corner[2]: (-0.4, 0.4)*cell_size.
+ * bg: background material triple. shapes, pmls: arrays of the structs above in
+ * device memory. paths: [npaths_total][2] (vertex start, count); verts: [nverts][2]
+ * float64. custom: [n][3] float64. pml_table: [n][2] float64. All pointers are
+ * device pointers. */
+int bz_rasterize2d(int32_t nx, int32_t ny, const double* xc, const double* yc,
+                   const double* offs, const double* corner, const double* bg,
+                   const bz_shape2d* shapes, int32_t n_shapes,
+                   const int32_t* paths, const double* verts, const double* custom,
+                   const bz_pml2d* pmls, int32_t n_pml, const double* pml_table,
+                   double dx, double eps0, double mu0,
+                   double* eps, double* mu, double* sigma, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* BEAMZ_B200_H */

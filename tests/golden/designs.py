@@ -1,0 +1,66 @@
+"""Design builders shared by the golden-fixture generator and the tests.
+
+Each builder takes a module namespace ``bz`` that provides the beamz API (the
+reference package when fixtures are generated, ``beamz_b200`` in the tests) and
+builds the same design with the same calls, so both sides rasterise and step
+identical inputs.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+UM = 1e-6
+RES = 0.05 * UM  # 50 nm cells keep the fixtures small
+
+
+def raster_shapes(bz):
+    """Every rasteriser path: rectangle fast path (with partial cells), circle,
+    ring, circular bend (ring path), taper and negative-height rectangle (polygon
+    path), polygon with a hole, order-3 PML with a sigma factor."""
+    d = bz.Design(width=3.02 * UM, height=2.51 * UM, material=bz.Material(2.085), pml_size=0.4 * UM)
+    d += bz.Rectangle(position=(0.0, 1.13 * UM), width=1.6 * UM, height=0.27 * UM, material=bz.Material(12.25))
+    d += bz.Circle(position=(2.1 * UM, 0.9 * UM), radius=0.33 * UM, material=bz.Material(6.0))
+    d += bz.Ring(position=(1.2 * UM, 0.75 * UM), inner_radius=0.21 * UM, outer_radius=0.42 * UM,
+                 material=bz.Material(9.0, 1.0, 0.0))
+    d += bz.CircularBend(position=(2.4 * UM, 2.0 * UM), inner_radius=0.2 * UM, outer_radius=0.35 * UM, angle=120,
+                         rotation=30, material=bz.Material(4.0))
+    d += bz.Taper(position=(0.55 * UM, 1.95 * UM), input_width=0.5 * UM, output_width=0.12 * UM,
+                  length=0.9 * UM, material=bz.Material(7.5))
+    d += bz.Rectangle(position=(1.9 * UM, 2.4 * UM), width=0.3 * UM, height=-0.6 * UM, material=bz.Material(3.3))
+    d += bz.Polygon(vertices=[(0.3 * UM, 0.3 * UM), (1.0 * UM, 0.45 * UM), (0.85 * UM, 0.95 * UM),
+                              (0.35 * UM, 0.8 * UM)],
+                    interiors=[[(0.5 * UM, 0.5 * UM), (0.7 * UM, 0.55 * UM), (0.6 * UM, 0.7 * UM)]],
+                    material=bz.Material(5.0, 1.0, 0.0))
+    d += bz.Rectangle(position=(1.45 * UM, 0.12 * UM), width=0.37 * UM, height=0.33 * UM,
+                      material=bz.Material(2.5, 1.0, 1e3))
+    for b in d.boundaries:
+        b.polynomial_order = 3
+        b.sigma_factor = 1.151
+    return d
+
+
+def raster_pml_only(bz):
+    """Vacuum box with the default (order-2) automatic PML."""
+    return bz.Design(width=2.0 * UM, height=1.5 * UM, pml_size=0.35 * UM)
+
+
+def wg_design(bz):
+    """Straight Si waveguide in SiO2 for the stepping fixtures."""
+    d = bz.Design(width=2.4 * UM, height=2.0 * UM, material=bz.Material(2.085), pml_size=0.4 * UM)
+    d += bz.Rectangle(position=(0.0, 0.8 * UM), width=2.4 * UM, height=0.4 * UM, material=bz.Material(12.25))
+    return d
+
+
+def time_axis(bz, n_steps, res=RES):
+    dt = 0.99 * res / (bz.LIGHT_SPEED * np.sqrt(2))
+    return np.arange(n_steps) * dt
+
+
+def gauss_signal(bz, t):
+    return bz.gaussian_pulse(t, 1.0, 6e-15, 2e-15, bz.LIGHT_SPEED / (1.55 * UM), 0.0) \
+        if hasattr(bz, "gaussian_pulse") else None
+
+
+def cw_signal(bz, t):
+    return bz.ramped_cosine(t, amplitude=1.0, frequency=bz.LIGHT_SPEED / (1.55 * UM), phase=0,
+                            ramp_duration=5e-15, t_max=t[-1])

@@ -1,0 +1,137 @@
+"""Generate the golden fixtures in this directory by running the reference beamz.
+
+Run in a container where the reference source tree is available:
+
+    python tests/golden/make_golden.py /path/to/beamz-reference
+
+The reference is imported from that path with stand-ins for its plotting/GDS
+imports (matplotlib, mpl_toolkits, gdspy are not installed and are not on the
+simulation path), and its own NumPy backend (float64 / complex128) produces:
+
+* raster_*.npz   RegularGrid permittivity / permeability / conductivity
+* step_*.npz     final Ez/Hx/Hy, monitor samples, power history and accumulated
+                 power of short 2D runs (Gaussian source; mode sources with the
+                 injected profile exported, since ARPACK's phase is arbitrary)
+* modes.npz      slab_mode_source profiles and solve_modes effective indices
+* signals.npz    ramped_cosine / gaussian_pulse samples
+
+The tests rebuild the same designs through beamz_b200 (``designs.py``) and compare.
+"""
+from __future__ import annotations
+
+import sys
+import types
+from pathlib import Path
+from unittest.mock import MagicMock
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+sys.path.insert(0, str(HERE))
+import designs as D  # noqa: E402
+
+
+def import_reference(path: str):
+    for m in ["matplotlib", "matplotlib.pyplot", "matplotlib.patches", "matplotlib.path", "matplotlib.animation",
+              "mpl_toolkits", "mpl_toolkits.mplot3d", "gdspy"]:
+        sys.modules.setdefault(m, MagicMock())
+    sys.path.insert(0, path)
+    import beamz
+    from beamz.devices import signals
+    from beamz.devices.mode import slab_mode_source, solve_modes
+    from beamz.simulation.meshing import RegularGrid
+
+    ns = {k: getattr(beamz, k) for k in dir(beamz) if not k.startswith("_")}
+    ns.update(gaussian_pulse=signals.gaussian_pulse, ramped_cosine=signals.ramped_cosine, RegularGrid=RegularGrid,
+              slab_mode_source=slab_mode_source, solve_modes=solve_modes)
+    return types.SimpleNamespace(**ns)
+
+
+def gauss_run(bz, n_steps=160):
+    d = D.wg_design(bz)
+    t = D.time_axis(bz, n_steps)
+    sig = D.gauss_signal(bz, t)
+    d += bz.GaussianSource(position=(1.2 * D.UM, 1.0 * D.UM), width=0.1 * D.UM, signal=sig)
+    mons = [bz.Monitor(design=d, start=(1.8 * D.UM, 0.5 * D.UM), end=(1.8 * D.UM, 1.5 * D.UM), name="v"),
+            bz.Monitor(design=d, start=(0.4 * D.UM, 1.6 * D.UM), end=(2.0 * D.UM, 1.6 * D.UM), name="h",
+                       record_interval=3),
+            bz.Monitor(design=d, start=(2.3 * D.UM, 0.1 * D.UM), end=(2.45 * D.UM, 1.9 * D.UM), name="edge")]
+    for m in mons:
+        d += m
+    return d, t, mons
+
+
+def mode_run(bz, n_steps=200, direction="+x", enforce=True):
+    d = D.wg_design(bz)
+    t = D.time_axis(bz, n_steps)
+    sig = D.cw_signal(bz, t)
+    if direction == "+x":
+        src = bz.ModeSource(design=d, start=(0.6 * D.UM, 0.45 * D.UM), end=(0.6 * D.UM, 1.55 * D.UM),
+                            wavelength=1.55 * D.UM, signal=sig, direction="+x", num_modes=1)
+        mon = bz.Monitor(design=d, start=(1.9 * D.UM, 0.5 * D.UM), end=(1.9 * D.UM, 1.5 * D.UM), name="out")
+    else:
+        src = bz.ModeSource(design=d, position=(1.2 * D.UM, 1.5 * D.UM), width=1.0 * D.UM,
+                            wavelength=1.55 * D.UM, signal=sig, direction="-y", num_modes=1)
+        mon = bz.Monitor(design=d, start=(0.7 * D.UM, 0.6 * D.UM), end=(1.7 * D.UM, 0.6 * D.UM), name="out")
+    if not enforce:
+        src.enforce_direction = False
+    d += src
+    d += mon
+    return d, t, src, [mon]
+
+
+def _pack_monitor(prefix, m, out):
+    for k in ("Ez", "Hx", "Hy"):
+        out[f"{prefix}_{k}"] = np.array([np.asarray(v, dtype=complex) for v in m.fields[k]])
+    out[f"{prefix}_t"] = np.asarray(m.fields["t"], dtype=float)
+    out[f"{prefix}_power"] = np.asarray(m.power_history)
+
+
+def run_and_pack(bz, d, t, mons, extra=None):
+    sim = bz.FDTD(design=d, time=t, mesh="regular", resolution=D.RES, backend="numpy")
+    sim.run(live=False, save=False, save_memory_mode=True, accumulate_power=True)
+    out = dict(Ez=np.asarray(sim.Ez), Hx=np.asarray(sim.Hx), Hy=np.asarray(sim.Hy),
+               power=np.asarray(sim.power_accumulated), eps=sim.mesh.permittivity, sigma=sim.mesh.conductivity)
+    for i, m in enumerate(mons):
+        _pack_monitor(f"m{i}", m, out)
+    if extra:
+        out.update(extra)
+    return out
+
+
+def main(ref_path: str):
+    bz = import_reference(ref_path)
+    for name, builder in (("shapes", D.raster_shapes), ("pml_only", D.raster_pml_only)):
+        g = bz.RegularGrid(builder(bz), D.RES)
+        np.savez_compressed(HERE / f"raster_{name}.npz", eps=g.permittivity, mu=g.permeability, sigma=g.conductivity)
+
+    d, t, mons = gauss_run(bz)
+    np.savez_compressed(HERE / "step_gauss.npz", **run_and_pack(bz, d, t, mons))
+    for tag, direction, enforce in (("mode_x", "+x", True), ("mode_y", "-y", False)):
+        d, t, src, mons = mode_run(bz, direction=direction, enforce=enforce)
+        prof = src.mode_profiles[0]
+        extra = dict(prof_amp=np.array([p[0] for p in prof], dtype=complex),
+                     prof_x=np.array([p[1] for p in prof]), prof_y=np.array([p[2] for p in prof]))
+        np.savez_compressed(HERE / f"step_{tag}.npz", **run_and_pack(bz, d, t, mons, extra))
+
+    x = np.linspace(-1.5e-6, 1.5e-6, 301)
+    modes = {}
+    for k, (w, n1, n0, m) in enumerate([(0.5e-6, 3.5, 1.444, 0), (0.5e-6, 2.25, 1.444, 0), (2.0e-6, 3.5, 1.444, 1),
+                                        (2.0e-6, 3.5, 1.444, 2)]):
+        E, ne = bz.slab_mode_source(x=x, w=w, n_WG=n1, n0=n0, wavelength=1.55e-6, ind_m=m)
+        modes[f"slab{k}_E"] = E
+        modes[f"slab{k}_neff"] = ne
+    eps1d = np.where(np.abs(np.linspace(-1e-6, 1e-6, 400)) < 0.25e-6, 12.25, 2.085)
+    neff, vecs = bz.solve_modes(eps1d, 2 * np.pi * bz.LIGHT_SPEED / 1.55e-6, 2e-6 / 400, npml=20, m=2)
+    modes.update(solve_neff=neff, solve_abs=np.abs(vecs), solve_eps=eps1d)
+    np.savez_compressed(HERE / "modes.npz", x=x, **modes)
+
+    tt = np.linspace(0, 60e-15, 500)
+    np.savez_compressed(HERE / "signals.npz", t=tt,
+                        ramped=bz.ramped_cosine(tt, 1.0, 1.9e14, phase=0.3, ramp_duration=8e-15, t_max=60e-15),
+                        pulse=bz.gaussian_pulse(tt, 1.3, 20e-15, 5e-15, 1.9e14, 0.1))
+    print("fixtures written to", HERE)
+
+
+if __name__ == "__main__":
+    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")

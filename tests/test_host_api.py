@@ -1,0 +1,152 @@
+"""Host-side parts of the API against the reference (no GPU): mode solvers,
+signals, PML profile, source compilation, topology helpers and Adam."""
+import numpy as np
+import pytest
+
+import make_golden as MG
+from designs import RES
+from oracle import fdtd2d
+
+
+def test_slab_mode_source_bit_exact(bz, golden):
+    g = golden("modes")
+    for k, (w, n1, n0, m) in enumerate([(0.5e-6, 3.5, 1.444, 0), (0.5e-6, 2.25, 1.444, 0), (2.0e-6, 3.5, 1.444, 1),
+                                        (2.0e-6, 3.5, 1.444, 2)]):
+        E, ne = bz.slab_mode_source(x=g["x"], w=w, n_WG=n1, n0=n0, wavelength=1.55e-6, ind_m=m)
+        np.testing.assert_array_equal(E, g[f"slab{k}_E"])
+        assert ne == g[f"slab{k}_neff"]
+
+
+def test_solve_modes_matches_up_to_phase(bz, golden):
+    g = golden("modes")
+    neff, vecs = bz.solve_modes(g["solve_eps"], 2 * np.pi * bz.LIGHT_SPEED / 1.55e-6, 2e-6 / 400, npml=20, m=2)
+    order = np.argsort(-np.real(neff))
+    gorder = np.argsort(-np.real(g["solve_neff"]))
+    np.testing.assert_allclose(neff[order], g["solve_neff"][gorder], rtol=1e-10)
+    np.testing.assert_allclose(np.abs(vecs[:, order]), g["solve_abs"][:, gorder], rtol=1e-6, atol=1e-9)
+
+
+def test_signals_bit_exact(bz, golden):
+    from beamz_b200.devices.signals import gaussian_pulse, ramped_cosine
+
+    g = golden("signals")
+    t = g["t"]
+    np.testing.assert_array_equal(ramped_cosine(t, 1.0, 1.9e14, phase=0.3, ramp_duration=8e-15, t_max=60e-15),
+                                  g["ramped"])
+    np.testing.assert_array_equal(gaussian_pulse(t, 1.3, 20e-15, 5e-15, 1.9e14, 0.1), g["pulse"])
+
+
+def test_stability_and_params(bz):
+    res, dt = bz.calc_optimal_fdtd_params(1.55e-6, 2.25, dims=2, safety_factor=0.99, points_per_wavelength=9)
+    ok, c, lim = bz.check_fdtd_stability(dt, res, dy=res)
+    assert ok and c == pytest.approx(0.99 / np.sqrt(2))
+
+
+def _apply_ops(ops, ez, step, n_comp):
+    """Apply compiled source ops to a flat field copy (the kernel's post phase)."""
+    out = ez.copy()
+    for c, m, w, s in zip(ops.cell, ops.mul, ops.weight, ops.sig):
+        val = ops.signals[s, step]
+        out[c] = m * out[c] + (w[0] + 1j * w[1]) * val
+    return out
+
+
+@pytest.mark.parametrize("case", ["gauss", "mode_x", "mode_y"])
+def test_compiled_source_ops_equal_sequential_injection(bz, golden, case):
+    """The merged per-cell operations give the reference's point-by-point result."""
+    from beamz_b200.simulation.compile_ops import compile_sources
+
+    if case == "gauss":
+        d, t, _ = MG.gauss_run(bz)
+    else:
+        d, t, src, _ = MG.mode_run(bz, direction="+x" if case == "mode_x" else "-y", enforce=case == "mode_x")
+        g = golden(f"step_{case}")
+        src.mode_profiles[0] = [[a, x, y, 0.0] for a, x, y in zip(g["prof_amp"], g["prof_x"], g["prof_y"])]
+    ny, nx = 40, 48
+    ops = compile_sources(d.sources, (ny, nx), (RES, RES), len(t))
+    rng = np.random.default_rng(0)
+    for step in (3, 77):
+        ez = rng.standard_normal((ny, nx)) + 1j * rng.standard_normal((ny, nx))
+        want = ez.copy()
+        for s in d.sources:
+            inj = fdtd2d._ModeInjector(s, RES, RES, nx, ny) if hasattr(s, "mode_profiles") else \
+                fdtd2d._GaussInjector(s, RES, RES, nx, ny)
+            inj.apply(want, step)
+        got = _apply_ops(ops, ez.ravel(), step, 2).reshape(ny, nx)
+        np.testing.assert_allclose(got, want, rtol=1e-13, atol=1e-13 * np.abs(want).max())
+
+
+def test_compiled_ops_enforce_zero_then_add_order(bz):
+    """A zeroed cell that is injected later keeps only the later injections."""
+    from beamz_b200.simulation.compile_ops import compile_sources
+
+    class Src:
+        direction = "+x"
+        enforce_direction = True
+        signal = np.ones(4)
+        mode_profiles = [[[1.0, 2 * RES, 1 * RES, 0], [2.0, 3 * RES, 1 * RES, 0], [5.0, 2 * RES, 1 * RES, 0]]]
+
+    from beamz_b200.devices.sources import ModeSource
+
+    s = ModeSource.__new__(ModeSource)
+    s.__dict__.update({k: getattr(Src, k) for k in ("direction", "enforce_direction", "signal", "mode_profiles")})
+    ops = compile_sources([s], (4, 6), (RES, RES), 4)
+    ez = np.arange(24, dtype=complex) + 10
+    got = _apply_ops(ops, ez, 1, 1).reshape(4, 6)
+    want = ez.reshape(4, 6).copy()
+    want[1, 2] += 1.0; want[1, 1] = 0  # noqa: E702
+    want[1, 3] += 2.0; want[1, 2] = 0  # noqa: E702
+    want[1, 2] += 5.0; want[1, 1] = 0  # noqa: E702
+    np.testing.assert_allclose(got, want)
+
+
+# ---- topology helpers: the reference's own tests (tests/test_topology_updates.py) ----
+
+def test_apply_density_update_changes_masked_region():
+    from beamz_b200.optimization.topology import apply_density_update
+
+    density = np.zeros((3, 3))
+    mask = np.zeros_like(density, dtype=bool)
+    mask[1, 1] = True
+    new, applied, delta, norm, mx = apply_density_update(density, np.ones_like(density), mask, learning_rate=0.2)
+    assert pytest.approx(new[1, 1]) == 0.2
+    assert norm > 0.0 and pytest.approx(mx) == norm
+    assert np.all(new[~mask] == 0.0) and np.all(delta[~mask] == 0.0)
+    assert applied[1, 1] == pytest.approx(1.0)
+
+
+def test_apply_density_update_obeys_clip_and_mask():
+    from beamz_b200.optimization.topology import apply_density_update
+
+    density = np.full((3, 3), 0.95)
+    mask = np.zeros_like(density, dtype=bool)
+    mask[1, 1] = True
+    new, _, delta, norm, mx = apply_density_update(density, np.ones_like(density), mask, learning_rate=0.5)
+    assert pytest.approx(new[1, 1]) == 1.0
+    assert np.all(new[~mask] == density[~mask]) and np.all(delta[~mask] == 0.0)
+    assert norm == pytest.approx(mx)
+
+
+def test_apply_density_update_zero_gradient_returns_no_change():
+    from beamz_b200.optimization.topology import apply_density_update
+
+    density = np.random.default_rng(1).random((4, 4))
+    mask = np.ones_like(density, dtype=bool)
+    new, applied, delta, norm, mx = apply_density_update(density, np.zeros_like(density), mask, learning_rate=0.3)
+    assert np.allclose(new, density) and np.allclose(applied, 0.0) and np.allclose(delta, 0.0)
+    assert norm == 0.0 and mx == 0.0
+
+
+def test_masked_blur_and_adam():
+    from beamz_b200.optimization.optimizers import Optimizer
+    from beamz_b200.optimization.topology import _masked_box_blur
+
+    v = np.arange(25.0).reshape(5, 5)
+    m = np.ones((5, 5), bool)
+    b = _masked_box_blur(v, m, 1)
+    assert b[2, 2] == pytest.approx(12.0)
+    opt = Optimizer(learning_rate=0.1)
+    u = opt.step(np.array([1.0, -2.0]))
+    np.testing.assert_allclose(u, [-0.1, 0.1], rtol=1e-6)
+    with pytest.raises(ValueError):
+        Optimizer(method="sgd")
