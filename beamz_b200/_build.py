@@ -1,6 +1,8 @@
 """Build libbeamz_b200.so in-tree with nvcc for sm_100a.
 
-Usage: ``python -m beamz_b200._build`` (also called by ``__graft_entry__.build``).
+Usage: ``python beamz_b200/_build.py [--force]`` (also called by
+``__graft_entry__.build``; it is loaded by path so that building never imports
+the package, whose import loads the library being built).
 Each ``csrc/*.cu`` file is compiled to an object under ``beamz_b200/_build/`` and
 linked into ``beamz_b200/libbeamz_b200.so``. Objects are rebuilt only when a
 source or header is newer.

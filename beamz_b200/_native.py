@@ -39,7 +39,7 @@ i32, i64, f64, vp = C.c_int32, C.c_int64, C.c_double, C.c_void_p
 
 class Grid2D(C.Structure):
     _fields_ = [("nx", i32), ("ny", i32), ("pitch", i32), ("n_designs", i32), ("n_comp", i32), ("n_mat", i32),
-                ("dtype", i32), ("reserved", i32), ("chx", f64), ("chy", f64), ("qy", f64), ("inv_kd2", f64)]
+                ("dtype", i32), ("tile_rows", i32), ("chx", f64), ("chy", f64), ("qy", f64), ("inv_kd2", f64)]
 
 
 class Fields2D(C.Structure):
@@ -52,8 +52,8 @@ class SourceOps(C.Structure):
 
 
 class MonitorOps(C.Structure):
-    _fields_ = [("n_points", i32), ("n_freq", i32), ("row_ptr", vp), ("cell", vp), ("point", vp), ("record", vp),
-                ("rec_step0", i64), ("n_rec", i32), ("n_phasor", i32), ("dft", vp), ("phasor", vp)]
+    _fields_ = [("n_points", i32), ("ring_len", i32), ("row_ptr", vp), ("cell", vp), ("point", vp), ("record", vp),
+                ("rec_step0", i64), ("n_rec", i32), ("reserved", i32), ("ring", vp)]
 
 
 class Shape2D(C.Structure):
@@ -79,6 +79,7 @@ _version = _sig("bz_version", C.c_char_p, [])
 _last_error = _sig("bz_last_error", C.c_int, [C.c_char_p, C.c_size_t])
 _step2d = _sig("bz_step2d", C.c_int, [C.POINTER(Grid2D), C.POINTER(Fields2D), C.POINTER(SourceOps),
                                        C.POINTER(MonitorOps), i64, vp, vp])
+_dft_fold = _sig("bz_dft_fold", C.c_int, [vp, i32, i32, i64, i32, vp, i64, i64, i32, vp, vp])
 _advance = _sig("bz_advance_step", C.c_int, [vp, i64, vp])
 _prepare = _sig("bz_prepare_coeffs", C.c_int, [vp, vp, i64, i32, i32, i32, f64, f64, f64, vp, vp, vp])
 _upd_h2d = _sig("bz_update_h2d", C.c_int, [i32, i32, i32, i32, vp, vp, vp, vp, f64, f64, f64, f64, f64, vp])
@@ -87,7 +88,7 @@ _raster2d = _sig("bz_rasterize2d", C.c_int, [i32, i32, vp, vp, vp, vp, vp, vp, i
                                               f64, f64, f64, vp, vp, vp, vp])
 
 #: every symbol include/beamz_b200.h declares (checked by the CPU test suite)
-EXPORTED = ["bz_version", "bz_last_error", "bz_step2d", "bz_advance_step", "bz_prepare_coeffs", "bz_update_h2d",
+EXPORTED = ["bz_version", "bz_last_error", "bz_step2d", "bz_dft_fold", "bz_advance_step", "bz_prepare_coeffs", "bz_update_h2d",
             "bz_update_e2d", "bz_rasterize2d"]
 
 
@@ -136,3 +137,7 @@ def update_h2d(*args) -> None:
 
 def update_e2d(*args) -> None:
     check(_upd_e2d(*args))
+
+
+def dft_fold(*args) -> None:
+    check(_dft_fold(*args))

@@ -17,6 +17,7 @@ from ..const import EPS_0, MU_0
 from .compile_ops import SourceOps, compile_monitors_2d, compile_sources
 
 GRAPH_CHUNK = 64  # steps per captured graph (even: keeps ping-pong parity)
+RING_LEN = GRAPH_CHUNK  # monitor samples kept between DFT folds
 
 
 def _round_up(n: int, m: int) -> int:
@@ -25,7 +26,7 @@ def _round_up(n: int, m: int) -> int:
 
 class Engine2D:
     def __init__(self, eps_r, sigma, dx, dy, dt, n_steps, sources, monitors, *, precision="fp32", n_comp=None,
-                 power=False, n_designs=1, record=True, use_graphs=True, device=None):
+                 power=False, n_designs=1, record=True, use_graphs=True, device=None, tile_rows=16):
         if not torch.cuda.is_available():
             raise RuntimeError("beamz_b200 needs a CUDA GPU (sm_100a); none is visible")
         self.dev = torch.device("cuda", torch.cuda.current_device()) if device is None else torch.device(device)
@@ -67,6 +68,7 @@ class Engine2D:
         g = nat.Grid2D()
         g.nx, g.ny, g.pitch = self.nx, self.ny, self.pitch
         g.n_designs, g.n_comp, g.n_mat, g.dtype = n_designs, n_comp, self.n_mat, self.bz_dtype
+        g.tile_rows = int(tile_rows)
         # x-differences use dy and y-differences dx, as the reference pairs them
         g.chx = self.dt / (MU_0 * self.dy)
         g.chy = self.dt / (MU_0 * self.dx)
@@ -92,8 +94,8 @@ class Engine2D:
         if len(s.cell) == 0:
             self.sops.n_ops = 0
             return
-        if self.n_comp == 1 and s.complex_weights:
-            raise ValueError("complex source amplitudes need n_comp=2")
+        # n_comp = 1 with complex amplitudes carries Re(field), the physical field:
+        # the update is real-linear, so the real part evolves on its own.
         t = lambda a, dt: self._kept(torch.as_tensor(np.ascontiguousarray(a)).to(self.dev, dt))  # noqa: E731
         self._src_t = dict(row=t(s.row_ptr, torch.int32), cell=t(s.cell, torch.int32),
                            mul=t(s.mul, self.dtype), w=t(s.weight[:, :self.n_comp], self.dtype),
@@ -116,6 +118,8 @@ class Engine2D:
         self.freqs = np.zeros(0)
         self.record = None
         self.dft = None
+        self.ring = None
+        self._folded = 0
         if self.mp.n_points == 0 or len(self.mp.cell) == 0:
             return
         mp = self.mp
@@ -142,9 +146,11 @@ class Engine2D:
             te, th = (n[:, None] + 1.0) * self.dt, (n[:, None] + 0.5) * self.dt
             ph = np.stack([np.cos(w * te), -np.sin(w * te), np.cos(w * th), -np.sin(w * th)], axis=-1)
             self.phasor = self._kept(torch.as_tensor(np.ascontiguousarray(ph)).to(self.dev))
+            self.ring = torch.zeros((RING_LEN, self.n_designs, self.n_comp, mp.n_points, 5), dtype=self.dtype,
+                                    device=self.dev)
             self.dft = torch.zeros((self.n_designs, self.n_comp, mp.n_points, nf, 5, 2), dtype=torch.float64,
                                    device=self.dev)
-            mo.n_freq, mo.dft, mo.phasor, mo.n_phasor = nf, self.dft.data_ptr(), self.phasor.data_ptr(), self.n_steps
+            mo.ring, mo.ring_len = self.ring.data_ptr(), RING_LEN
         self._rec_host: list[np.ndarray] = []
         self._rec_first = 0
 
@@ -177,6 +183,33 @@ class Engine2D:
         self._maybe_drain()
         self._launch(self.step_index, None)
         self.step_index += 1
+        if self.dft is not None and self.step_index - self._folded >= RING_LEN:
+            self._fold()
+
+    def _fold(self):
+        """Fold the monitor samples of steps [folded, step_index) into the DFT sums."""
+        while self.dft is not None and self._folded < self.step_index:
+            cnt = min(RING_LEN, self.step_index - self._folded)
+            nat.dft_fold(self.ring.data_ptr(), self.bz_dtype, RING_LEN, self.n_designs * self.n_comp * self.mp.n_points,
+                         len(self.freqs), self.phasor.data_ptr(), self.n_steps, self._folded, cnt,
+                         self.dft.data_ptr(), self._stream())
+            self._folded += cnt
+
+    def reset(self):
+        """Zero the fields and accumulators and rewind to step 0 (material and
+        compiled operations are kept)."""
+        for bufs in (self.ez, self.hx, self.hy):
+            for b in bufs:
+                b.zero_()
+        for t in (self.dft, self.power, self.ring):
+            if t is not None:
+                t.zero_()
+        self.step_index = 0
+        self._folded = 0
+        if self.record is not None:
+            self._rec_host = []
+            self.mops.rec_step0 = 0
+            self._graphs.clear()
 
     def _graph_for(self, phase: int) -> torch.cuda.CUDAGraph:
         """Graph of GRAPH_CHUNK launches starting at a step of parity `phase`; the
@@ -207,6 +240,7 @@ class Engine2D:
                 g.replay()
                 self.step_index += GRAPH_CHUNK
                 n -= GRAPH_CHUNK
+                self._fold()
                 continue
             self.step_once()
             n -= 1
@@ -256,6 +290,7 @@ class Engine2D:
         """DFT sums times dt, complex [designs][comp][points][freq][5]."""
         if self.dft is None:
             return None
+        self._fold()
         a = self.dft.cpu().numpy()
         self.d2h_bytes += a.nbytes
         return (a[..., 0] + 1j * a[..., 1]) * self.dt

@@ -118,7 +118,7 @@ class FDTD:
 
             self.engine = Engine2D(self.mesh.permittivity, self.mesh.conductivity, self.dx, self.dy, self.dt,
                                    self.num_steps, self.sources, self.monitors, precision=precision, n_comp=n_comp,
-                                   power=accumulate_power, use_graphs=graphs)
+                                   power=accumulate_power, use_graphs=graphs, tile_rows=opts.get("tile_rows", 16))
 
     def __getattr__(self, name):
         # field access with the reference's names and shapes (device tensors)
@@ -234,8 +234,11 @@ class FDTD:
         if hasattr(eng, "collect_monitors"):
             eng.collect_monitors(recs, times)
             return
-        if recs is None:
-            return
+        if recs is not None:
+            self._load_records(eng, recs, times, steps)
+        self._collect_dft()
+
+    def _load_records(self, eng, recs, times, steps):
         for mon, sl, ok in zip(eng.mp.monitors, eng.mp.slices, eng.mp.valid):
             part = recs[:, 0, :, sl, :]  # [steps][comp][points][3]
             vals = part[:, 0] + 1j * part[:, 1] if eng.n_comp == 2 else part[:, 0]
@@ -248,7 +251,6 @@ class FDTD:
                 ez, hx, hy = ez.astype(np.complex128), hx.astype(np.complex128), hy.astype(np.complex128)
             mon.load_record_2d(ez, hx, hy, times[sel])
             mon.last_record_step = int(sel[-1]) if len(sel) else mon.last_record_step
-        self._collect_dft()
 
     def _collect_dft(self):
         eng = self.engine

@@ -49,6 +49,7 @@ def parse():
     p.add_argument("--time-steps", type=int, default=None, help="override the workload's step count")
     p.add_argument("--cpu-steps", type=int, default=60, help="time steps of the CPU baseline sample")
     p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--n-comp", type=int, default=1, help="field components: 1 = real (physical) field, 2 = Re+Im")
     return p.parse_args()
 
 
@@ -167,21 +168,13 @@ def run_b200(args):
     ny, nx = grid.permittivity.shape
     cells = nx * ny
     n_steps = len(t)
-    sim = FDTD(design=grid, time=t)
+    sim = FDTD(design=grid, time=t, backend_options={"n_comp": args.n_comp})
     sim.initialize_simulation(save=False, live=False, save_memory_mode=True)
     eng = sim.engine
     flush = torch.empty(512 << 20, dtype=torch.uint8, device="cuda")
 
-    def reset():
-        for bufs in (eng.ez, eng.hx, eng.hy):
-            for b in bufs:
-                b.zero_()
-        if eng.dft is not None:
-            eng.dft.zero_()
-        eng.step_index = 0
-
     def one_run(evs=None):
-        reset()
+        eng.reset()
         flush.fill_(1)
         if evs is not None:
             evs[0].record()
@@ -219,7 +212,7 @@ def run_b200(args):
 
     # dominant kernel: the fused step launch (one per time step)
     per_launch_s = sum(run_ms) * 1e-3 / (args.steps * n_steps)
-    algo_bytes = BYTES_PER_CELL_2D * cells
+    algo_bytes = (24 * args.n_comp + 8) * cells  # fields r+w per component + ce, loss
     peak, peak_kind = measured_peaks()
     achieved = algo_bytes / per_launch_s / 1e9
     traffic = profiled_traffic("step2d", args.workload)
@@ -282,7 +275,7 @@ def run_e2e(grid, t, cells, n_steps, args, world):
     for k in range(max(1, min(args.steps, 3))):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        sim = FDTD(design=grid, time=t)
+        sim = FDTD(design=grid, time=t, backend_options={"n_comp": args.n_comp})
         sim.run(live=False, save=False, save_memory_mode=True)
         torch.cuda.synchronize()
         times.append(time.perf_counter() - t0)

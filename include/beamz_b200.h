@@ -70,7 +70,7 @@ typedef struct bz_grid2d {
   int32_t nx, ny, pitch;
   int32_t n_designs, n_comp, n_mat;
   int32_t dtype;
-  int32_t reserved;
+  int32_t tile_rows;        /* rows per thread block: 4, 8, 16 or 32 (0 = 16) */
   double chx, chy, qy, inv_kd2;
 } bz_grid2d;
 
@@ -107,24 +107,24 @@ typedef struct bz_source_ops {
 
 /* Monitor sampling after injection (monitors.py:279-315). Each point samples,
  * at its cell: Ez, Hx, Hy (the reference's record_fields_2d triple) and, for the
- * DFT, the two neighbours used to centre H on the E node.
+ * frequency-domain monitors, the two staggered neighbours used to centre H on
+ * the E node.
  * record (optional): [n_rec][n_designs][n_comp][n_points][3] dtype, row
  *   (step - rec_step0) for rec_step0 <= step < rec_step0 + n_rec.
- * dft (optional, float64): [n_designs][n_comp][n_points][n_freq][5][2] running sums of
- *   q * exp(-i w t) for q in (Ez, Hx(x), Hx(x-1), Hy(y), Hy(y-1)); phasor[step][f] =
- *   (cos wtE, -sin wtE, cos wtH, -sin wtH) with tE = (step+1)dt, tH = (step+1/2)dt. */
+ * ring (optional): [ring_len][n_designs][n_comp][n_points][5] dtype, slot
+ *   step % ring_len, holding (Ez, Hx(x), Hx(x-1), Hy(y), Hy(y-1)); folded into
+ *   float64 DFT sums by bz_dft_fold at least every ring_len steps. */
 typedef struct bz_monitor_ops {
   int32_t n_points;
-  int32_t n_freq;
+  int32_t ring_len;
   const int32_t* row_ptr;   /* [rows+1] as in bz_source_ops */
   const int32_t* cell;      /* [n_points] sorted ascending */
   const int32_t* point;     /* [n_points] output slot of each sorted entry */
   void* record;
   int64_t rec_step0;
   int32_t n_rec;
-  int32_t n_phasor;         /* rows of phasor; steps beyond it accumulate nothing */
-  double* dft;
-  const double* phasor;
+  int32_t reserved;
+  void* ring;
 } bz_monitor_ops;
 
 /* One full time step of the 2D Ez-mode Yee scheme for every design and component:
@@ -136,6 +136,17 @@ typedef struct bz_monitor_ops {
  * copy read stays (step & 1). */
 int bz_step2d(const bz_grid2d* g, const bz_fields2d* f, const bz_source_ops* src,
               const bz_monitor_ops* mon, int64_t step, const int64_t* d_step, void* stream);
+
+/* Folds `count` consecutive ring samples, steps step0 .. step0+count-1 (ring slot
+ * step % ring_len, count <= ring_len), into float64 DFT sums:
+ *   dft[i][f][q] += sum_s ring[s % ring_len][i][q] * phasor[s][f][E or H]
+ * for i < n_items (= designs*components*points), q < 5 (q = 0 uses the E phasor,
+ * q >= 1 the H phasor). phasor[s][f] = (cos wt_E, -sin wt_E, cos wt_H, -sin wt_H)
+ * with t_E = (s+1) dt and t_H = (s+1/2) dt; dft is [n_items][n_freq][5][2]. Steps at
+ * or beyond n_phasor contribute nothing. One warp per (item, frequency) reduces
+ * over the steps with shuffles. */
+int bz_dft_fold(const void* ring, int32_t dtype, int32_t ring_len, int64_t n_items, int32_t n_freq,
+                const double* phasor, int64_t n_phasor, int64_t step0, int32_t count, double* dft, void* stream);
 
 /* Adds n to the device step counter (*d_step += n). */
 int bz_advance_step(int64_t* d_step, int64_t n, void* stream);

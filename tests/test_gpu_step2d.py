@@ -163,3 +163,15 @@ def test_tiny_grid_rejected(bz):
     with pytest.raises(ValueError):
         sim = bz.FDTD(design=d, time=np.arange(4) * 1e-17, resolution=1e-8)
         sim.run(live=False)
+
+
+@pytest.mark.parametrize("rows", [4, 8, 32])
+def test_tile_heights_agree(bz, rows):
+    eps, sigma, dx, dt, t, sig, _ = _random_problem(13, ny=45, nx=70, n_steps=150)
+    src = bz.GaussianSource(position=(30 * dx, 20 * dx), width=dx / 10, signal=sig)
+    outs = []
+    for tr in (16, rows):
+        sim = _sim_from_arrays(bz, eps, sigma, dx, t, [src], [], "fp32", tile_rows=tr)
+        sim.run(live=False, save=False, save_memory_mode=True)
+        outs.append(sim.engine.field("Ez").cpu().numpy())
+    assert rel_l2(outs[1], outs[0]) <= 1e-6
