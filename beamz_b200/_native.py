@@ -80,6 +80,9 @@ _last_error = _sig("bz_last_error", C.c_int, [C.c_char_p, C.c_size_t])
 _step2d = _sig("bz_step2d", C.c_int, [C.POINTER(Grid2D), C.POINTER(Fields2D), C.POINTER(SourceOps),
                                        C.POINTER(MonitorOps), i64, vp, vp])
 _dft_fold = _sig("bz_dft_fold", C.c_int, [vp, i32, i32, i64, i32, vp, i64, i64, i32, vp, vp])
+_step2d_dft_static = _sig("bz_step2d_dft_static", C.c_int,
+                          [C.POINTER(Grid2D), C.POINTER(Fields2D), C.POINTER(SourceOps), C.POINTER(MonitorOps), i64,
+                           i32, i32, vp, i64, vp, vp])
 _advance = _sig("bz_advance_step", C.c_int, [vp, i64, vp])
 _prepare = _sig("bz_prepare_coeffs", C.c_int, [vp, vp, i64, i32, i32, i32, f64, f64, f64, vp, vp, vp])
 _upd_h2d = _sig("bz_update_h2d", C.c_int, [i32, i32, i32, i32, vp, vp, vp, vp, f64, f64, f64, f64, f64, vp])
@@ -88,7 +91,7 @@ _raster2d = _sig("bz_rasterize2d", C.c_int, [i32, i32, vp, vp, vp, vp, vp, vp, i
                                               f64, f64, f64, vp, vp, vp, vp])
 
 #: every symbol include/beamz_b200.h declares (checked by the CPU test suite)
-EXPORTED = ["bz_version", "bz_last_error", "bz_step2d", "bz_dft_fold", "bz_advance_step", "bz_prepare_coeffs", "bz_update_h2d",
+EXPORTED = ["bz_version", "bz_last_error", "bz_step2d", "bz_dft_fold", "bz_step2d_dft_static", "bz_advance_step", "bz_prepare_coeffs", "bz_update_h2d",
             "bz_update_e2d", "bz_rasterize2d"]
 
 

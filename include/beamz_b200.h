@@ -148,6 +148,21 @@ int bz_step2d(const bz_grid2d* g, const bz_fields2d* f, const bz_source_ops* src
 int bz_dft_fold(const void* ring, int32_t dtype, int32_t ring_len, int64_t n_items, int32_t n_freq,
                 const double* phasor, int64_t n_phasor, int64_t step0, int32_t count, double* dft, void* stream);
 
+/* Allocation-free variant of bz_step2d + bz_dft_fold for callers that cannot call
+ * cudaMalloc (for example a binding whose runtime owns all device memory through its
+ * own pool, or a host with a fixed device-memory budget). No counterpart in the
+ * reference: it has no frequency-domain monitors and no device memory management.
+ * Runs n_steps steps from step0 (direct launches) and folds the monitors' samples into
+ * dft ([n_designs*n_comp*n_points][n_freq][5][2], float64) exactly as bz_dft_fold does,
+ * keeping the sample ring in an 8 MiB array compiled into the library instead of
+ * mon->ring, which must be NULL. One step of samples (n_designs*n_comp*n_points*5
+ * elements of dtype) must fit in 8 MiB; larger requests return BZ_ERR_INVALID. The
+ * first call on a device looks up the array's address (make it before any stream
+ * capture). All calls share the array; calls that overlap on the GPU race. */
+int bz_step2d_dft_static(const bz_grid2d* g, const bz_fields2d* f, const bz_source_ops* src,
+                         const bz_monitor_ops* mon, int64_t step0, int32_t n_steps, int32_t n_freq,
+                         const double* phasor, int64_t n_phasor, double* dft, void* stream);
+
 /* Adds n to the device step counter (*d_step += n). */
 int bz_advance_step(int64_t* d_step, int64_t n, void* stream);
 
