@@ -64,3 +64,29 @@ def gauss_signal(bz, t):
 def cw_signal(bz, t):
     return bz.ramped_cosine(t, amplitude=1.0, frequency=bz.LIGHT_SPEED / (1.55 * UM), phase=0,
                             ramp_duration=5e-15, t_max=t[-1])
+
+
+def design_3d(bz):
+    """Small 3D stack: substrate slab, strip waveguide, a disc (3D rasteriser paths)."""
+    d = bz.Design(width=1.5 * UM, height=1.2 * UM, depth=0.8 * UM, material=bz.Material(1.0), pml_size=0.2 * UM)
+    d += bz.Rectangle(position=(0, 0, 0), width=1.5 * UM, height=1.2 * UM, depth=0.4 * UM, material=bz.Material(2.085))
+    d += bz.Rectangle(position=(0, 0.45 * UM, 0.4 * UM), width=1.5 * UM, height=0.3 * UM, depth=0.22 * UM,
+                      material=bz.Material(12.25))
+    d += bz.Circle(position=(1.0 * UM, 0.6 * UM, 0.4 * UM), radius=0.2 * UM, material=bz.Material(6.0))
+    return d
+
+
+def step3d_design(bz):
+    return bz.Design(width=0.85 * UM, height=0.75 * UM, depth=0.65 * UM, material=bz.Material(1.0), pml_size=0.1 * UM)
+
+
+def step3d_arrays(shape, seed=5):
+    rng = np.random.default_rng(seed)
+    nz, ny, nx = shape
+    zz, yy, xx = np.meshgrid(np.arange(nz), np.arange(ny), np.arange(nx), indexing="ij")
+    eps = 1.0 + 5.0 * (1 + np.sin(0.7 * xx + 0.3 * yy) * np.cos(0.5 * zz)) + rng.random(shape)
+    sig = np.zeros(shape)
+    for a, n in ((xx, nx), (yy, ny), (zz, nz)):
+        d = np.maximum(0, np.maximum(3 - a, a - (n - 4))) / 3.0
+        sig += 4e4 * d ** 3
+    return eps, sig

@@ -14,6 +14,9 @@ simulation path), and its own NumPy backend (float64 / complex128) produces:
                  injected profile exported, since ARPACK's phase is arbitrary)
 * modes.npz      slab_mode_source profiles and solve_modes effective indices
 * signals.npz    ramped_cosine / gaussian_pulse samples
+* raster3d.npz   RegularGrid3D output (the reference's own 3D rasteriser)
+* step3d.npz     final six field components, z-normal plane monitor records and
+                 accumulated power of a short 3D run on prescribed eps/sigma
 
 The tests rebuild the same designs through beamz_b200 (``designs.py``) and compare.
 """
@@ -39,10 +42,11 @@ def import_reference(path: str):
     import beamz
     from beamz.devices import signals
     from beamz.devices.mode import slab_mode_source, solve_modes
-    from beamz.simulation.meshing import RegularGrid
+    from beamz.simulation.meshing import RegularGrid, RegularGrid3D
 
     ns = {k: getattr(beamz, k) for k in dir(beamz) if not k.startswith("_")}
     ns.update(gaussian_pulse=signals.gaussian_pulse, ramped_cosine=signals.ramped_cosine, RegularGrid=RegularGrid,
+              RegularGrid3D=RegularGrid3D,
               slab_mode_source=slab_mode_source, solve_modes=solve_modes)
     return types.SimpleNamespace(**ns)
 
@@ -99,6 +103,32 @@ def run_and_pack(bz, d, t, mons, extra=None):
     return out
 
 
+def step3d_run(bz, n_steps=60):
+    """Small 3D run on prescribed eps/sigma (copied into the mesh, as examples/4_topo.py
+    does in 2D): Gaussian source, 3D mode source plane, two plane monitors."""
+    d = D.step3d_design(bz)
+    res = D.RES
+    grid = bz.RegularGrid3D(d, res)
+    eps, sig = D.step3d_arrays(grid.permittivity.shape)
+    np.copyto(grid.permittivity, eps)
+    np.copyto(grid.conductivity, sig)
+    dt = 0.99 * res / (bz.LIGHT_SPEED * np.sqrt(3))
+    t = np.arange(n_steps) * dt
+    sg = bz.gaussian_pulse(t, 1.0, 10 * dt, 4 * dt, bz.LIGHT_SPEED / (1.55 * D.UM), 0.0)
+    cw = bz.ramped_cosine(t, amplitude=1.0, frequency=bz.LIGHT_SPEED / (1.55 * D.UM), phase=0,
+                          ramp_duration=8 * dt, t_max=t[-1])
+    g = bz.GaussianSource(position=(0.4 * D.UM, 0.35 * D.UM, 0.3 * D.UM), width=0.06 * D.UM, signal=sg)
+    m = bz.ModeSource(design=d, position=(0.25 * D.UM, 0.38 * D.UM, 0.33 * D.UM), width=0.3 * D.UM,
+                      height=0.25 * D.UM, wavelength=1.55 * D.UM, signal=cw, direction="+x", num_modes=1)
+    mz = bz.Monitor(design=d, start=(0.1 * D.UM, 0.1 * D.UM, 0.32 * D.UM), end=(0.7 * D.UM, 0.6 * D.UM, 0.32 * D.UM))
+    # only z-normal planes: the reference's x/y-normal plane slicing falls back to whole arrays and fails
+    mx = bz.Monitor(design=d, start=(0.2 * D.UM, 0.05 * D.UM, 0.45 * D.UM), end=(0.8 * D.UM, 0.7 * D.UM, 0.45 * D.UM),
+                    record_interval=2)
+    for dev in (g, m, mz, mx):  # through the design: the reference's devices= path fails for GaussianSource
+        d += dev
+    return d, grid, t, [g, m], [mz, mx]
+
+
 def main(ref_path: str):
     bz = import_reference(ref_path)
     for name, builder in (("shapes", D.raster_shapes), ("pml_only", D.raster_pml_only)):
@@ -113,6 +143,23 @@ def main(ref_path: str):
         extra = dict(prof_amp=np.array([p[0] for p in prof], dtype=complex),
                      prof_x=np.array([p[1] for p in prof]), prof_y=np.array([p[2] for p in prof]))
         np.savez_compressed(HERE / f"step_{tag}.npz", **run_and_pack(bz, d, t, mons, extra))
+
+    g3 = bz.RegularGrid3D(D.design_3d(bz), D.RES)
+    np.savez_compressed(HERE / "raster3d.npz", eps=g3.permittivity, mu=g3.permeability, sigma=g3.conductivity)
+    d, grid, t, srcs, mons = step3d_run(bz)
+    sim = bz.FDTD(design=grid, time=t, backend="numpy")
+    sim.run(live=False, save=False, save_memory_mode=True, accumulate_power=True)
+    out = {k: np.asarray(getattr(sim, k)) for k in ("Ex", "Ey", "Ez", "Hx", "Hy", "Hz")}
+    out["power"] = np.asarray(sim.power_accumulated)
+    prof = srcs[1].mode_profiles[0]
+    amps = np.array([p[0] for p in prof], dtype=complex)  # deterministic (analytic slab modes): summarised only
+    out.update(prof_n=len(prof), prof_sum=amps.sum(), prof_xyz_sum=np.array([p[1:4] for p in prof]).sum(axis=0))
+    for i, m in enumerate(mons):
+        for k in ("Ex", "Ey", "Ez", "Hx", "Hy", "Hz"):
+            out[f"m{i}_{k}"] = np.array(m.fields[k])
+        out[f"m{i}_t"] = np.asarray(m.fields["t"], dtype=float)
+        out[f"m{i}_power"] = np.asarray(m.power_history)
+    np.savez_compressed(HERE / "step3d.npz", **out)
 
     x = np.linspace(-1.5e-6, 1.5e-6, 301)
     modes = {}

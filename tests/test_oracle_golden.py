@@ -54,3 +54,49 @@ def test_oracle_rasteriser_matches_reference(bz, golden, name):
     np.testing.assert_array_equal(eps, g["eps"])
     np.testing.assert_array_equal(mu, g["mu"])
     np.testing.assert_array_equal(sig, g["sigma"])
+
+
+def _step3d_setup(bz, golden):
+    import designs as D
+
+    g = golden("step3d")
+    d = D.step3d_design(bz)
+    nz, ny, nx = int(0.65e-6 / D.RES), int(0.75e-6 / D.RES), int(0.85e-6 / D.RES)
+    eps, sig = D.step3d_arrays((nz, ny, nx))
+    res = D.RES
+    dt = 0.99 * res / (bz.LIGHT_SPEED * np.sqrt(3))
+    t = np.arange(60) * dt
+    sg = bz.gaussian_pulse(t, 1.0, 10 * dt, 4 * dt, bz.LIGHT_SPEED / (1.55e-6), 0.0)
+    cw = bz.ramped_cosine(t, amplitude=1.0, frequency=bz.LIGHT_SPEED / 1.55e-6, phase=0, ramp_duration=8 * dt,
+                          t_max=t[-1])
+    src_g = bz.GaussianSource(position=(0.4e-6, 0.35e-6, 0.3e-6), width=0.06e-6, signal=sg)
+    src_m = bz.ModeSource(design=d, position=(0.25e-6, 0.38e-6, 0.33e-6), width=0.3e-6, height=0.25e-6,
+                          wavelength=1.55e-6, signal=cw, direction="+x", num_modes=1)
+    mz = bz.Monitor(design=d, start=(0.1e-6, 0.1e-6, 0.32e-6), end=(0.7e-6, 0.6e-6, 0.32e-6))
+    mx = bz.Monitor(design=d, start=(0.2e-6, 0.05e-6, 0.45e-6), end=(0.8e-6, 0.7e-6, 0.45e-6), record_interval=2)
+    for dev in (src_g, src_m, mz, mx):
+        d += dev
+    return g, d, eps, sig, res, dt, t, [src_g, src_m], [mz, mx]
+
+
+def test_mode_source_3d_profile_matches_reference(bz, golden):
+    g, d, eps, sig, res, dt, t, srcs, mons = _step3d_setup(bz, golden)
+    prof = srcs[1].mode_profiles[0]
+    assert len(prof) == int(g["prof_n"])
+    assert np.sum(np.array([p[0] for p in prof], dtype=complex)) == g["prof_sum"]
+    np.testing.assert_array_equal(np.array([p[1:4] for p in prof]).sum(axis=0), g["prof_xyz_sum"])
+
+
+def test_oracle_3d_matches_reference_run(bz, golden):
+    from oracle import fdtd3d
+
+    g, d, eps, sig, res, dt, t, srcs, mons = _step3d_setup(bz, golden)
+    out = fdtd3d.run(eps, sig, res, res, res, dt, len(t), srcs, mons, accumulate_power=True)
+    for k in ("Ex", "Ey", "Ez", "Hx", "Hy", "Hz"):
+        np.testing.assert_array_equal(out["fields"][k], g[k])
+    np.testing.assert_allclose(out["power"], g["power"] * len(t), rtol=1e-12)
+    for i, rec in enumerate(out["records"]):
+        for k in ("Ex", "Ey", "Ez", "Hx", "Hy", "Hz"):
+            np.testing.assert_array_equal(rec["fields"][k], g[f"m{i}_{k}"])
+        np.testing.assert_array_equal(rec["t"], g[f"m{i}_t"])
+        np.testing.assert_array_equal(rec["power"], g[f"m{i}_power"])
