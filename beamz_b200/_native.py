@@ -56,12 +56,32 @@ class MonitorOps(C.Structure):
                 ("rec_step0", i64), ("n_rec", i32), ("reserved", i32), ("ring", vp)]
 
 
+class Grid3D(C.Structure):
+    _fields_ = [("nx", i32), ("ny", i32), ("nz", i32), ("pitch", i32), ("n_designs", i32), ("n_comp", i32),
+                ("n_mat", i32), ("dtype", i32), ("tile_z", i32), ("reserved", i32), ("chx", f64), ("chy", f64),
+                ("chz", f64), ("qx", f64), ("qz", f64), ("inv_kd2", f64)]
+
+
+class Fields3D(C.Structure):
+    _fields_ = [("e", (vp * 3) * 2), ("h", (vp * 3) * 2), ("ce", vp), ("loss", vp)]
+
+
+class GatherOps(C.Structure):
+    _fields_ = [("n_points", i32), ("n_q", i32), ("src", vp * 6), ("offset", vp), ("record", vp), ("rec_step0", i64),
+                ("n_rec", i32), ("ring_len", i32), ("ring", vp)]
+
+
 class Shape2D(C.Structure):
     _fields_ = [("kind", i32), ("i0", i32), ("i1", i32), ("j0", i32), ("j1", i32), ("fill", i32), ("fi0", i32),
                 ("fi1", i32), ("fj0", i32), ("fj1", i32), ("top", i32), ("bottom", i32), ("left", i32),
                 ("right", i32), ("path0", i32), ("npath", i32), ("custom_off", i32), ("reserved", i32),
                 ("p0", f64), ("p1", f64), ("p2", f64), ("p3", f64), ("q", f64), ("perm", f64), ("permb", f64),
                 ("cond", f64)]
+
+
+class Shape3D(C.Structure):
+    _fields_ = [("i0", i32), ("i1", i32), ("j0", i32), ("j1", i32), ("k0", i32), ("k1", i32), ("path0", i32),
+                ("npath", i32), ("zw_off", i32), ("reserved", i32), ("perm", f64), ("permb", f64), ("cond", f64)]
 
 
 class Pml2D(C.Structure):
@@ -83,6 +103,13 @@ _dft_fold = _sig("bz_dft_fold", C.c_int, [vp, i32, i32, i64, i32, vp, i64, i64, 
 _step2d_dft_static = _sig("bz_step2d_dft_static", C.c_int,
                           [C.POINTER(Grid2D), C.POINTER(Fields2D), C.POINTER(SourceOps), C.POINTER(MonitorOps), i64,
                            i32, i32, vp, i64, vp, vp])
+_step3d = _sig("bz_step3d", C.c_int, [C.POINTER(Grid3D), C.POINTER(Fields3D), i64, vp])
+_cell_ops = _sig("bz_cell_ops", C.c_int, [vp, i32, i32, i32, i64, i32, i32, C.POINTER(SourceOps), i64, vp, vp])
+_gather = _sig("bz_gather", C.c_int, [C.POINTER(GatherOps), i32, i32, i32, i64, i64, vp, vp])
+_power3d = _sig("bz_power3d", C.c_int, [C.POINTER(Grid3D), C.POINTER(Fields3D), i32, vp, vp])
+_dft_fold_q = _sig("bz_dft_fold_q", C.c_int, [vp, i32, i32, i64, i32, i32, i32, vp, i64, i64, i32, vp, vp])
+_raster3d = _sig("bz_rasterize3d", C.c_int, [i32, i32, i32, i32, vp, vp, vp, vp, vp, i32, vp, vp, vp, vp, i32, vp,
+                                              vp, f64, f64, f64, f64, vp, vp, vp, vp])
 _advance = _sig("bz_advance_step", C.c_int, [vp, i64, vp])
 _prepare = _sig("bz_prepare_coeffs", C.c_int, [vp, vp, i64, i32, i32, i32, f64, f64, f64, vp, vp, vp])
 _upd_h2d = _sig("bz_update_h2d", C.c_int, [i32, i32, i32, i32, vp, vp, vp, vp, f64, f64, f64, f64, f64, vp])
@@ -91,7 +118,8 @@ _raster2d = _sig("bz_rasterize2d", C.c_int, [i32, i32, vp, vp, vp, vp, vp, vp, i
                                               f64, f64, f64, vp, vp, vp, vp])
 
 #: every symbol include/beamz_b200.h declares (checked by the CPU test suite)
-EXPORTED = ["bz_version", "bz_last_error", "bz_step2d", "bz_dft_fold", "bz_step2d_dft_static", "bz_advance_step", "bz_prepare_coeffs", "bz_update_h2d",
+EXPORTED = ["bz_version", "bz_last_error", "bz_step2d", "bz_dft_fold", "bz_step2d_dft_static", "bz_advance_step",
+            "bz_step3d", "bz_cell_ops", "bz_gather", "bz_power3d", "bz_dft_fold_q", "bz_rasterize3d", "bz_prepare_coeffs", "bz_update_h2d",
             "bz_update_e2d", "bz_rasterize2d"]
 
 
@@ -144,3 +172,27 @@ def update_e2d(*args) -> None:
 
 def dft_fold(*args) -> None:
     check(_dft_fold(*args))
+
+
+def step3d(grid, fields, step, stream) -> None:
+    check(_step3d(C.byref(grid), C.byref(fields), step, stream))
+
+
+def cell_ops(field, dtype, n_designs, n_comp, comp_stride, nx, pitch, ops, step, d_step, stream) -> None:
+    check(_cell_ops(field, dtype, n_designs, n_comp, comp_stride, nx, pitch, C.byref(ops), step, d_step, stream))
+
+
+def gather(ops, dtype, n_designs, n_comp, comp_stride, step, d_step, stream) -> None:
+    check(_gather(C.byref(ops), dtype, n_designs, n_comp, comp_stride, step, d_step, stream))
+
+
+def power3d(grid, fields, cur, power, stream) -> None:
+    check(_power3d(C.byref(grid), C.byref(fields), cur, power, stream))
+
+
+def dft_fold_q(*args) -> None:
+    check(_dft_fold_q(*args))
+
+
+def rasterize3d(*args) -> None:
+    check(_raster3d(*args))

@@ -219,3 +219,86 @@ extern "C" int bz_rasterize2d(int32_t nx, int32_t ny, const double* xc, const do
                                                                      pml_table, dx, eps0, mu0, eps, mu, sigma);
   return bz::check_launch("bz_rasterize2d");
 }
+
+namespace bz {
+namespace {
+
+__device__ __forceinline__ double pml_term(double eps, double prof, double ff, double sf, double dx, double eps0,
+                                           double mu0) {
+  const double eta = __dsqrt_rn(fdiv(mu0, fmul(eps0, eps)));
+  double smax = fdiv(1.2, fmul(eta, dx));
+  smax = fmul(smax, sf);
+  return fmul(fmul(smax, prof), ff);
+}
+
+__global__ void rasterize3d_kernel(int nx, int ny, int nz, int n_zs, const double* __restrict__ xc,
+                                   const double* __restrict__ yc, const double* __restrict__ offs,
+                                   const double* __restrict__ bg, const bz_shape3d* __restrict__ shapes, int n_shapes,
+                                   const int* __restrict__ zw, const int* __restrict__ paths,
+                                   const double* __restrict__ verts, const bz_pml2d* __restrict__ pmls, int n_pml,
+                                   const double* __restrict__ pml_table, const double* __restrict__ prof_z,
+                                   double sf_z, double dx, double eps0, double mu0, double* __restrict__ eps_out,
+                                   double* __restrict__ mu_out, double* __restrict__ sig_out) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = blockIdx.y * blockDim.y + threadIdx.y;
+  const int k = blockIdx.z;
+  if (i >= ny || j >= nx) return;
+  const double X = xc[j], Y = yc[i];
+  double e = bg[0], m = bg[1], c = bg[2];
+  const double o0 = offs[0], o1 = offs[1], o2 = offs[2];
+  const double sx[9] = {fadd(X, o0), fadd(X, o1), fadd(X, o2), fadd(X, o0), fadd(X, o1),
+                        fadd(X, o2), fadd(X, o0), fadd(X, o1), fadd(X, o2)};
+  const double sy[9] = {fadd(Y, o0), fadd(Y, o0), fadd(Y, o0), fadd(Y, o1), fadd(Y, o1),
+                        fadd(Y, o1), fadd(Y, o2), fadd(Y, o2), fadd(Y, o2)};
+  for (int s_i = 0; s_i < n_shapes; ++s_i) {
+    const bz_shape3d s = shapes[s_i];
+    if (k < s.k0 || k >= s.k1 || i < s.i0 || i >= s.i1 || j < s.j0 || j >= s.j1) continue;
+    const int w = zw[s.zw_off + (k - s.k0)];
+    if (w == 0) continue;
+    bz_shape2d p;
+    p.path0 = s.path0;
+    p.npath = s.npath;
+    int cnt = 0;
+    for (int t = 0; t < 9; ++t) cnt += in_polygon(sx[t], sy[t], p, paths, verts);
+    if (cnt > 0) blend(e, m, c, fdiv((double)(cnt * w), (double)(9 * n_zs)), s.perm, s.permb, s.cond);
+  }
+  for (int b = 0; b < n_pml; ++b) {
+    const bz_pml2d p = pmls[b];
+    if (i < p.i0 || i >= p.i1 || j < p.j0 || j >= p.j1) continue;
+    const long long idx = p.table_off + (long long)(i - p.i0) * (p.j1 - p.j0) + (j - p.j0);
+    const double prof = pml_table[2 * idx], ff = pml_table[2 * idx + 1];
+    if (prof < 0.0) continue;
+    const double cond = pml_term(e, prof, ff, p.sigma_factor, dx, eps0, mu0);
+    if (cond > 0.0) c = fadd(c, cond);
+  }
+  if (prof_z != nullptr && prof_z[2 * k] >= 0.0) {
+    const double cond = pml_term(e, prof_z[2 * k], prof_z[2 * k + 1], sf_z, dx, eps0, mu0);
+    if (cond > 0.0) c = fadd(c, cond);
+  }
+  const long long o = ((long long)k * ny + i) * nx + j;
+  eps_out[o] = e;
+  mu_out[o] = m;
+  sig_out[o] = c;
+}
+
+}  // namespace
+}  // namespace bz
+
+extern "C" int bz_rasterize3d(int32_t nx, int32_t ny, int32_t nz, int32_t n_zs, const double* xc, const double* yc,
+                              const double* offs, const double* bg, const bz_shape3d* shapes, int32_t n_shapes,
+                              const int32_t* zw, const int32_t* paths, const double* verts, const bz_pml2d* pmls,
+                              int32_t n_pml, const double* pml_table, const double* prof_z, double sigma_factor_z,
+                              double dx, double eps0, double mu0, double* eps, double* mu, double* sigma,
+                              void* stream) {
+  BZ_REQUIRE(nx >= 1 && ny >= 1 && nz >= 1 && nz <= 65535, "bz_rasterize3d: bad grid %d x %d x %d", nx, ny, nz);
+  BZ_REQUIRE(n_zs == 1 || n_zs == 3, "bz_rasterize3d: n_zs must be 1 or 3");
+  BZ_REQUIRE(xc && yc && offs && bg && eps && mu && sigma, "bz_rasterize3d: NULL buffer");
+  BZ_REQUIRE(n_shapes == 0 || (shapes && zw && paths && verts), "bz_rasterize3d: shape tables are NULL");
+  BZ_REQUIRE(n_pml == 0 || (pmls && pml_table), "bz_rasterize3d: PML tables are NULL");
+  dim3 block(32, 8);
+  dim3 grid((unsigned)bz::ceil_div(nx, 32), (unsigned)bz::ceil_div(ny, 8), (unsigned)nz);
+  bz::rasterize3d_kernel<<<grid, block, 0, bz::as_stream(stream)>>>(
+      nx, ny, nz, n_zs, xc, yc, offs, bg, shapes, n_shapes, zw, paths, verts, pmls, n_pml, pml_table, prof_z,
+      sigma_factor_z, dx, eps0, mu0, eps, mu, sigma);
+  return bz::check_launch("bz_rasterize3d");
+}

@@ -1,0 +1,414 @@
+// 3D Yee time step, fused H + E (beamz/simulation/fdtd.py:200-310), plus the
+// small kernels around it: source injection on one array (helper.py:5-118),
+// monitor gathers (helper.py:235-244, monitors.py:317-396) and |S| accumulation
+// (helper.py:124-151).
+//
+// Tiling of bz_step3d: a 32 x 8 thread block covers a 32 x 8 column patch whose
+// first column and first row are a halo shared with the neighbouring patch, so it
+// owns 31 x 7 columns; it marches along z over tile_z planes. Per plane:
+//   1. E(k) of the patch goes to shared memory (y+1 neighbours), x+1 neighbours
+//      come from the next lane by warp shuffle (lane 31 and row 7 read global);
+//   2. every thread computes H(k) (the halo row/column too);
+//   3. H(k) goes to shared memory (y-1 neighbours), x-1 neighbours by shuffle,
+//      H(k-1) is carried in registers from the previous plane;
+//   4. owned threads compute E(k) and write H(k), E(k).
+// The first plane's H(k-1) is recomputed from global memory. Ping-pong copies
+// keep every launch reading only the previous step's values.
+#include "bz_internal.cuh"
+
+namespace bz {
+namespace {
+
+constexpr unsigned FULL = 0xffffffffu;
+constexpr int TX = 32, TY = 8;
+
+template <typename T>
+struct Geo3D {
+  int nx, ny, nz, pitch, n_designs, n_mat, nzb;
+  long long plane, vol;  // ny*pitch, nz*plane
+  T chx, chy, chz, qx, qz, inv_kd2;
+};
+
+template <typename T>
+struct Ptr3 {
+  const T* e[3];
+  const T* h[3];
+};
+
+template <typename T>
+struct Out3 {
+  T* e[3];
+  T* h[3];
+};
+
+template <typename T>
+__device__ __forceinline__ void hfac(T a, const Geo3D<T>& g, T& fh, T& cx, T& cy, T& cz) {
+  if (a == T(0)) {
+    fh = T(1);
+    cx = g.chx;
+    cy = g.chy;
+    cz = g.chz;
+  } else {
+    const T den = T(1) + a;
+    fh = (T(1) - a) / den;
+    cx = g.chx / den;
+    cy = g.chy / den;
+    cz = g.chz / den;
+  }
+}
+
+template <typename T>
+__device__ __forceinline__ T ld(const T* p, long long i, bool ok) {
+  return ok ? __ldg(p + i) : T(0);
+}
+
+template <typename T, int NC, int ZB>
+__global__ void __launch_bounds__(TX * TY) step3d_kernel(Ptr3<T> in, Out3<T> out, const T* __restrict__ ce,
+                                                          const T* __restrict__ loss, Geo3D<T> g) {
+  __shared__ T s_ez[NC][TY][TX], s_ex[NC][TY][TX], s_hz[NC][TY][TX], s_hx[NC][TY][TX];
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  const int nx = g.nx, ny = g.ny, nz = g.nz;
+  const int x = blockIdx.x * (TX - 1) - 1 + tx;
+  const int y = blockIdx.y * (TY - 1) - 1 + ty;
+  const int d = blockIdx.z / g.nzb;
+  const int z0 = (blockIdx.z - d * g.nzb) * ZB;
+  const int z1 = min(z0 + ZB, nz);
+  const bool xin = x >= 0 && x < nx, yin = y >= 0 && y < ny, inb = xin && yin;
+  const bool owned = inb && tx >= 1 && ty >= 1;
+  const long long P = g.plane;
+  const long long mb = (g.n_mat > 1 ? (long long)d : 0LL) * g.vol;
+  const long long col = (long long)y * g.pitch + x;  // offset inside a plane
+  long long fb[NC];
+#pragma unroll
+  for (int c = 0; c < NC; ++c) fb[c] = ((long long)d * NC + c) * g.vol;
+
+  T exk[NC], eyk[NC], ezk[NC], hxm[NC], hym[NC];
+#pragma unroll
+  for (int c = 0; c < NC; ++c) {
+    const long long o = fb[c] + (long long)z0 * P + col;
+    exk[c] = ld(in.e[0], o, inb);
+    eyk[c] = ld(in.e[1], o, inb);
+    ezk[c] = ld(in.e[2], o, inb);
+    hxm[c] = T(0);
+    hym[c] = T(0);
+  }
+  if (z0 >= 1 && inb) {  // H(z0-1) at this column, recomputed from global memory
+    const int k = z0 - 1;
+    T fh, cx, cy, cz;
+    hfac(__ldg(loss + mb + (long long)k * P + col), g, fh, cx, cy, cz);
+#pragma unroll
+    for (int c = 0; c < NC; ++c) {
+      const long long o = fb[c] + (long long)k * P + col;
+      const T ez = __ldg(in.e[2] + o), ex = __ldg(in.e[0] + o), ey = __ldg(in.e[1] + o);
+      const T ez_yp = ld(in.e[2], o + g.pitch, y + 1 < ny);
+      const T ez_xp = ld(in.e[2], o + 1, x + 1 < nx);
+      const T ey_zp = eyk[c], ex_zp = exk[c];  // plane z0
+      hxm[c] = fh * __ldg(in.h[0] + o) - (cy * (ez_yp - ez) - cz * (ey_zp - ey));
+      hym[c] = fh * __ldg(in.h[1] + o) - (cz * (ex_zp - ex) - cx * (ez_xp - ez));
+    }
+  }
+
+  for (int k = z0; k < z1; ++k) {
+    const long long po = (long long)k * P + col;
+    const T a = ld(loss + mb, po, inb);
+    const T cev = ld(ce + mb, po, inb);
+    T fh, cx, cy, cz;
+    hfac(a, g, fh, cx, cy, cz);
+    const T fe = T(1) - a * cev * g.inv_kd2;
+    T exn[NC], eyn[NC], ezn[NC], hx0[NC], hy0[NC], hz0[NC];
+#pragma unroll
+    for (int c = 0; c < NC; ++c) {
+      const long long o = fb[c] + po;
+      exn[c] = ld(in.e[0], o + P, inb && k + 1 < nz);
+      eyn[c] = ld(in.e[1], o + P, inb && k + 1 < nz);
+      ezn[c] = ld(in.e[2], o + P, inb && k + 1 < nz);
+      hx0[c] = ld(in.h[0], o, inb);
+      hy0[c] = ld(in.h[1], o, inb);
+      hz0[c] = ld(in.h[2], o, inb);
+      s_ez[c][ty][tx] = ezk[c];
+      s_ex[c][ty][tx] = exk[c];
+    }
+    __syncthreads();
+    T hxn[NC], hyn[NC], hzn[NC];
+#pragma unroll
+    for (int c = 0; c < NC; ++c) {
+      const long long o = fb[c] + po;
+      T ez_yp, ex_yp;
+      if (ty < TY - 1) {
+        ez_yp = s_ez[c][ty + 1][tx];
+        ex_yp = s_ex[c][ty + 1][tx];
+      } else {
+        ez_yp = ld(in.e[2], o + g.pitch, xin && y + 1 < ny && y >= -1);
+        ex_yp = ld(in.e[0], o + g.pitch, xin && y + 1 < ny && y >= -1);
+      }
+      T ez_xp = __shfl_down_sync(FULL, ezk[c], 1);
+      T ey_xp = __shfl_down_sync(FULL, eyk[c], 1);
+      if (tx == TX - 1) {
+        ez_xp = ld(in.e[2], o + 1, yin && x + 1 < nx);
+        ey_xp = ld(in.e[1], o + 1, yin && x + 1 < nx);
+      }
+      hxn[c] = fh * hx0[c] - (cy * (ez_yp - ezk[c]) - cz * (eyn[c] - eyk[c]));
+      hyn[c] = fh * hy0[c] - (cz * (exn[c] - exk[c]) - cx * (ez_xp - ezk[c]));
+      hzn[c] = fh * hz0[c] - (cx * (ey_xp - eyk[c]) - cy * (ex_yp - exk[c]));
+      s_hz[c][ty][tx] = hzn[c];
+      s_hx[c][ty][tx] = hxn[c];
+    }
+    __syncthreads();
+#pragma unroll
+    for (int c = 0; c < NC; ++c) {
+      const T hy_xm = __shfl_up_sync(FULL, hyn[c], 1);
+      const T hz_xm = __shfl_up_sync(FULL, hzn[c], 1);
+      if (owned) {
+        const long long o = fb[c] + po;
+        const T hz_ym = s_hz[c][ty - 1][tx];
+        const T hx_ym = s_hx[c][ty - 1][tx];
+        const bool kin = k >= 1 && k <= nz - 2;
+        T ex = exk[c], ey = eyk[c], ez = ezk[c];
+        if (kin && y >= 1 && y <= ny - 2 && x <= nx - 2)
+          ex = fe * exk[c] + cev * ((hzn[c] - hz_ym) - g.qz * (hyn[c] - hym[c]));
+        if (kin && y <= ny - 2 && x >= 1 && x <= nx - 2)
+          ey = fe * eyk[c] + cev * (g.qz * (hxn[c] - hxm[c]) - g.qx * (hzn[c] - hz_xm));
+        if (k <= nz - 2 && y >= 1 && y <= ny - 2 && x >= 1 && x <= nx - 2)
+          ez = fe * ezk[c] + cev * (g.qx * (hyn[c] - hy_xm) - (hxn[c] - hx_ym));
+        if (x <= nx - 2) out.e[0][o] = ex;
+        if (y <= ny - 2) out.e[1][o] = ey;
+        if (k <= nz - 2) out.e[2][o] = ez;
+        if (k <= nz - 2 && y <= ny - 2) out.h[0][o] = hxn[c];
+        if (k <= nz - 2 && x <= nx - 2) out.h[1][o] = hyn[c];
+        if (y <= ny - 2 && x <= nx - 2) out.h[2][o] = hzn[c];
+      }
+      exk[c] = exn[c];
+      eyk[c] = eyn[c];
+      ezk[c] = ezn[c];
+      hxm[c] = hxn[c];
+      hym[c] = hyn[c];
+    }
+  }
+}
+
+template <typename T, int NC, int ZB>
+int launch3d(const bz_grid3d* gd, const bz_fields3d* f, int64_t step, cudaStream_t st) {
+  Geo3D<T> g;
+  g.nx = gd->nx;
+  g.ny = gd->ny;
+  g.nz = gd->nz;
+  g.pitch = gd->pitch;
+  g.n_designs = gd->n_designs;
+  g.n_mat = gd->n_mat;
+  g.nzb = (int)ceil_div(gd->nz, ZB);
+  g.plane = (long long)gd->ny * gd->pitch;
+  g.vol = g.plane * gd->nz;
+  g.chx = (T)gd->chx;
+  g.chy = (T)gd->chy;
+  g.chz = (T)gd->chz;
+  g.qx = (T)gd->qx;
+  g.qz = (T)gd->qz;
+  g.inv_kd2 = (T)gd->inv_kd2;
+  const int src = (int)(step & 1);
+  Ptr3<T> in;
+  Out3<T> out;
+  for (int i = 0; i < 3; ++i) {
+    in.e[i] = (const T*)f->e[src][i];
+    in.h[i] = (const T*)f->h[src][i];
+    out.e[i] = (T*)f->e[src ^ 1][i];
+    out.h[i] = (T*)f->h[src ^ 1][i];
+  }
+  dim3 block(TX, TY);
+  dim3 grid((unsigned)ceil_div(gd->nx, TX - 1), (unsigned)ceil_div(gd->ny, TY - 1), (unsigned)(g.nzb * gd->n_designs));
+  step3d_kernel<T, NC, ZB><<<grid, block, 0, st>>>(in, out, (const T*)f->ce, (const T*)f->loss, g);
+  return check_launch("bz_step3d");
+}
+
+template <typename T>
+int dispatch3d(const bz_grid3d* g, const bz_fields3d* f, int64_t step, cudaStream_t st) {
+  const bool z8 = g->tile_z == 8;
+  if (g->n_comp == 1) return z8 ? launch3d<T, 1, 8>(g, f, step, st) : launch3d<T, 1, 16>(g, f, step, st);
+  return z8 ? launch3d<T, 2, 8>(g, f, step, st) : launch3d<T, 2, 16>(g, f, step, st);
+}
+
+// ---------------------------------------------------------------------------- cell ops
+template <typename T>
+__global__ void cell_ops_kernel(T* __restrict__ field, int n_comp, long long comp_stride, int nx, int pitch,
+                                int n_ops, int n_steps, const int* __restrict__ cell, const T* __restrict__ mul,
+                                const T* __restrict__ w, const int* __restrict__ sig, const T* __restrict__ signals,
+                                long long step_base, const long long* __restrict__ d_step) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n_ops) return;
+  const int c0 = __ldg(cell + k);
+  if (k > 0 && __ldg(cell + k - 1) == c0) return;  // the first op of a cell applies its whole run
+  const long long step = d_step ? (__ldg(d_step) + step_base) : step_base;
+  const int d = blockIdx.y;
+  const long long off = (long long)(c0 / nx) * pitch + (c0 % nx);
+  for (int c = 0; c < n_comp; ++c) {
+    T* p = field + ((long long)d * n_comp + c) * comp_stride + off;
+    T v = *p;
+    for (int kk = k; kk < n_ops && __ldg(cell + kk) == c0; ++kk) {
+      const T s = step < n_steps ? __ldg(signals + (long long)__ldg(sig + kk) * n_steps + step) : T(0);
+      v = __ldg(mul + kk) * v + __ldg(w + (long long)kk * n_comp + c) * s;
+    }
+    *p = v;
+  }
+}
+
+// ---------------------------------------------------------------------------- gather
+template <typename T>
+struct GatherArgs {
+  int n_points, n_q, n_designs, n_comp, n_rec, ring_len;
+  const T* src[6];
+  const long long* offset;
+  T* record;
+  T* ring;
+  long long rec_step0, comp_stride;
+};
+
+template <typename T>
+__global__ void gather_kernel(GatherArgs<T> a, long long step_base, const long long* __restrict__ d_step) {
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;  // (point, q)
+  const long long total = (long long)a.n_points * a.n_q;
+  if (i >= total) return;
+  const long long step = d_step ? (__ldg(d_step) + step_base) : step_base;
+  const int p = (int)(i / a.n_q), q = (int)(i - (long long)p * a.n_q);
+  const long long off = __ldg(a.offset + i);
+  const int dc = blockIdx.y;  // design * n_comp + comp
+  const T v = off >= 0 ? __ldg(a.src[q] + dc * a.comp_stride + off) : T(0);
+  const long long tail = ((long long)dc * a.n_points + p) * a.n_q + q;
+  const long long per = (long long)a.n_designs * a.n_comp * a.n_points * a.n_q;
+  if (a.record && step >= a.rec_step0 && step < a.rec_step0 + a.n_rec) a.record[(step - a.rec_step0) * per + tail] = v;
+  if (a.ring) a.ring[(step % a.ring_len) * per + tail] = v;
+}
+
+// ---------------------------------------------------------------------------- power
+template <typename T, int NC>
+__global__ void power3d_kernel(Ptr3<T> f, Geo3D<T> g, double* __restrict__ pw) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y = blockIdx.y;
+  const int kd = blockIdx.z;  // design * (nz-1) + k
+  const int mz = g.nz - 1, my = g.ny - 1, mx = g.nx - 1;
+  if (x >= mx) return;
+  const int d = kd / mz, k = kd - d * mz;
+  const long long o = (long long)k * g.plane + (long long)y * g.pitch + x;
+  double sx = 0, sy = 0, sz = 0;
+  for (int c = 0; c < NC; ++c) {  // Re(a conj(b)) summed over the (re, im) parts
+    const long long b = ((long long)d * NC + c) * g.vol + o;
+    const double ex = __ldg(f.e[0] + b), ey = __ldg(f.e[1] + b), ez = __ldg(f.e[2] + b);
+    const double hx = __ldg(f.h[0] + b), hy = __ldg(f.h[1] + b), hz = __ldg(f.h[2] + b);
+    sx += ey * hz - ez * hy;
+    sy += ez * hx - ex * hz;
+    sz += ex * hy - ey * hx;
+  }
+  pw[(((long long)d * mz + k) * my + y) * mx + x] += sqrt(sx * sx + sy * sy + sz * sz);
+}
+
+}  // namespace
+}  // namespace bz
+
+extern "C" int bz_step3d(const bz_grid3d* g, const bz_fields3d* f, int64_t step, void* stream) {
+  BZ_REQUIRE(g && f, "bz_step3d: grid or fields is NULL");
+  BZ_REQUIRE(g->nx >= 2 && g->ny >= 2 && g->nz >= 2, "bz_step3d: grid must be at least 2x2x2");
+  BZ_REQUIRE(g->pitch >= g->nx && g->pitch % 32 == 0, "bz_step3d: pitch %d must be >= nx and a multiple of 32",
+             g->pitch);
+  BZ_REQUIRE(g->n_comp == 1 || g->n_comp == 2, "bz_step3d: n_comp must be 1 or 2");
+  BZ_REQUIRE(g->n_designs >= 1 && g->n_designs * bz::ceil_div(g->nz, 8) <= 65535, "bz_step3d: too many designs");
+  BZ_REQUIRE(g->n_mat == 1 || g->n_mat == g->n_designs, "bz_step3d: n_mat must be 1 or n_designs");
+  BZ_REQUIRE(g->tile_z == 0 || g->tile_z == 8 || g->tile_z == 16, "bz_step3d: tile_z must be 0, 8 or 16");
+  for (int c = 0; c < 2; ++c)
+    for (int i = 0; i < 3; ++i) BZ_REQUIRE(f->e[c][i] && f->h[c][i], "bz_step3d: field buffer is NULL");
+  BZ_REQUIRE(f->ce && f->loss, "bz_step3d: coefficient arrays are NULL");
+  BZ_REQUIRE(step >= 0, "bz_step3d: negative step");
+  cudaStream_t st = bz::as_stream(stream);
+  if (g->dtype == BZ_F32) return bz::dispatch3d<float>(g, f, step, st);
+  if (g->dtype == BZ_F64) return bz::dispatch3d<double>(g, f, step, st);
+  return bz::fail(BZ_ERR_INVALID, "bz_step3d: unknown dtype %d", g->dtype);
+}
+
+extern "C" int bz_cell_ops(void* field, int32_t dtype, int32_t n_designs, int32_t n_comp, int64_t comp_stride,
+                           int32_t nx, int32_t pitch, const bz_source_ops* ops, int64_t step, const int64_t* d_step,
+                           void* stream) {
+  BZ_REQUIRE(field && ops, "bz_cell_ops: NULL field or ops");
+  if (ops->n_ops == 0) return BZ_OK;
+  BZ_REQUIRE(ops->cell && ops->mul && ops->weight && ops->sig && ops->signals, "bz_cell_ops: incomplete ops");
+  BZ_REQUIRE(nx >= 1 && pitch >= nx && n_designs >= 1 && (n_comp == 1 || n_comp == 2), "bz_cell_ops: bad shape");
+  dim3 grid((unsigned)bz::ceil_div(ops->n_ops, 128), (unsigned)n_designs);
+  cudaStream_t st = bz::as_stream(stream);
+  if (dtype == BZ_F32)
+    bz::cell_ops_kernel<float><<<grid, 128, 0, st>>>((float*)field, n_comp, comp_stride, nx, pitch, ops->n_ops,
+                                                     ops->n_steps, ops->cell, (const float*)ops->mul,
+                                                     (const float*)ops->weight, ops->sig,
+                                                     (const float*)ops->signals, step, (const long long*)d_step);
+  else if (dtype == BZ_F64)
+    bz::cell_ops_kernel<double><<<grid, 128, 0, st>>>((double*)field, n_comp, comp_stride, nx, pitch, ops->n_ops,
+                                                      ops->n_steps, ops->cell, (const double*)ops->mul,
+                                                      (const double*)ops->weight, ops->sig,
+                                                      (const double*)ops->signals, step, (const long long*)d_step);
+  else
+    return bz::fail(BZ_ERR_INVALID, "bz_cell_ops: unknown dtype %d", dtype);
+  return bz::check_launch("bz_cell_ops");
+}
+
+template <typename T>
+static int gather_t(const bz_gather_ops* o, int32_t n_designs, int32_t n_comp, int64_t comp_stride, int64_t step,
+                    const int64_t* d_step, cudaStream_t st) {
+  bz::GatherArgs<T> a;
+  a.n_points = o->n_points;
+  a.n_q = o->n_q;
+  a.n_designs = n_designs;
+  a.n_comp = n_comp;
+  a.n_rec = o->n_rec;
+  a.ring_len = o->ring_len;
+  for (int q = 0; q < 6; ++q) a.src[q] = (const T*)o->src[q];
+  a.offset = (const long long*)o->offset;
+  a.record = (T*)o->record;
+  a.ring = (T*)o->ring;
+  a.rec_step0 = o->rec_step0;
+  a.comp_stride = comp_stride;
+  const long long total = (long long)o->n_points * o->n_q;
+  dim3 grid((unsigned)bz::ceil_div(total, 128), (unsigned)(n_designs * n_comp));
+  bz::gather_kernel<T><<<grid, 128, 0, st>>>(a, step, (const long long*)d_step);
+  return bz::check_launch("bz_gather");
+}
+
+extern "C" int bz_gather(const bz_gather_ops* o, int32_t dtype, int32_t n_designs, int32_t n_comp,
+                         int64_t comp_stride, int64_t step, const int64_t* d_step, void* stream) {
+  BZ_REQUIRE(o && o->offset, "bz_gather: NULL ops or offsets");
+  BZ_REQUIRE(o->n_q >= 1 && o->n_q <= 6 && o->n_points >= 0, "bz_gather: n_q must be 1..6");
+  for (int q = 0; q < o->n_q; ++q) BZ_REQUIRE(o->src[q], "bz_gather: source array %d is NULL", q);
+  BZ_REQUIRE(o->ring == nullptr || o->ring_len >= 1, "bz_gather: ring without length");
+  if (o->n_points == 0 || (!o->record && !o->ring)) return BZ_OK;
+  cudaStream_t st = bz::as_stream(stream);
+  if (dtype == BZ_F32) return gather_t<float>(o, n_designs, n_comp, comp_stride, step, d_step, st);
+  if (dtype == BZ_F64) return gather_t<double>(o, n_designs, n_comp, comp_stride, step, d_step, st);
+  return bz::fail(BZ_ERR_INVALID, "bz_gather: unknown dtype %d", dtype);
+}
+
+template <typename T>
+static int power_t(const bz_grid3d* gd, const bz_fields3d* f, int cur, double* pw, cudaStream_t st) {
+  bz::Geo3D<T> g = {};
+  g.nx = gd->nx;
+  g.ny = gd->ny;
+  g.nz = gd->nz;
+  g.pitch = gd->pitch;
+  g.plane = (long long)gd->ny * gd->pitch;
+  g.vol = g.plane * gd->nz;
+  bz::Ptr3<T> p;
+  for (int i = 0; i < 3; ++i) {
+    p.e[i] = (const T*)f->e[cur][i];
+    p.h[i] = (const T*)f->h[cur][i];
+  }
+  dim3 grid((unsigned)bz::ceil_div(gd->nx - 1, 128), (unsigned)(gd->ny - 1), (unsigned)(gd->n_designs * (gd->nz - 1)));
+  if (gd->n_comp == 1)
+    bz::power3d_kernel<T, 1><<<grid, 128, 0, st>>>(p, g, pw);
+  else
+    bz::power3d_kernel<T, 2><<<grid, 128, 0, st>>>(p, g, pw);
+  return bz::check_launch("bz_power3d");
+}
+
+extern "C" int bz_power3d(const bz_grid3d* g, const bz_fields3d* f, int32_t cur, double* power, void* stream) {
+  BZ_REQUIRE(g && f && power, "bz_power3d: NULL argument");
+  BZ_REQUIRE(cur == 0 || cur == 1, "bz_power3d: cur must be 0 or 1");
+  BZ_REQUIRE(g->nx >= 2 && g->ny >= 2 && g->nz >= 2 && (g->n_comp == 1 || g->n_comp == 2), "bz_power3d: bad shape");
+  BZ_REQUIRE((long long)g->n_designs * (g->nz - 1) <= 65535 && g->ny - 1 <= 65535, "bz_power3d: grid too large");
+  cudaStream_t st = bz::as_stream(stream);
+  if (g->dtype == BZ_F32) return power_t<float>(g, f, cur, power, st);
+  if (g->dtype == BZ_F64) return power_t<double>(g, f, cur, power, st);
+  return bz::fail(BZ_ERR_INVALID, "bz_power3d: unknown dtype %d", g->dtype);
+}

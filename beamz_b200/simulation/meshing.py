@@ -293,11 +293,26 @@ class RegularGrid(BaseMeshGrid):
         raise NotImplementedError("plotting is not part of beamz_b200")
 
 
-class RegularGrid3D(BaseMeshGrid):  # completed in the 3D module
+class RegularGrid3D(BaseMeshGrid):
+    """3D material grid [z, y, x] (meshing.py:569-893); see meshing3d for the two
+    rasterisation modes (reference semantics by default, ``extrude=True`` for the
+    physically extruded stack)."""
+
     def __init__(self, design, resolution_xy=None, resolution_z=None, **kwargs):
         from .meshing3d import init_regular_grid_3d
 
         init_regular_grid_3d(self, design, resolution_xy, resolution_z, **kwargs)
+
+    def get_2d_slice(self, z_index=None, z_position=None):
+        if z_index is None and z_position is None:
+            z_index = self.shape[0] // 2
+        elif z_position is not None:
+            z_index = max(0, min(self.shape[0] - 1, int(z_position / self.resolution_z)))
+        return {"permittivity": self.permittivity[z_index], "permeability": self.permeability[z_index],
+                "conductivity": self.conductivity[z_index]}
+
+    def show(self, *args, **kwargs):
+        raise NotImplementedError("plotting is not part of beamz_b200")
 
 
 def create_mesh(design, resolution, auto_select=True, force_3d=False):

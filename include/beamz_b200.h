@@ -188,6 +188,72 @@ int bz_update_e2d(int32_t dtype, int32_t ny, int32_t nx, int32_t nc, void* ez, c
                   const void* sigma, const void* eps_r, double dx, double dy, double dt, double eps0, void* stream);
 
 /* ----------------------------------------------------------------------------
+ * 3D Yee scheme (beamz/simulation/fdtd.py:200-310). Every component is stored as
+ * [n_designs][n_comp][nz][ny][pitch] (x contiguous); positions outside a
+ * component's reference shape (Ex (nz, ny, nx-1), Ey (nz, ny-1, nx),
+ * Ez (nz-1, ny, nx), Hx (nz-1, ny-1, nx), Hy (nz-1, ny, nx-1), Hz (nz, ny-1, nx-1))
+ * stay zero.
+ *   chx, chy, chz  dt/(mu0*dx), dt/(mu0*dy), dt/(mu0*dz)
+ *   qx, qz         dy/dx, dy/dz (E curl weights relative to the y-difference)
+ *   inv_kd2        2*eps0*dy/dt (ce and loss as in bz_prepare_coeffs with dy)
+ * -------------------------------------------------------------------------- */
+typedef struct bz_grid3d {
+  int32_t nx, ny, nz, pitch;
+  int32_t n_designs, n_comp, n_mat, dtype;
+  int32_t tile_z;           /* z planes per thread block: 8 or 16 (0 = 16) */
+  int32_t reserved;
+  double chx, chy, chz, qx, qz, inv_kd2;
+} bz_grid3d;
+
+typedef struct bz_fields3d {
+  void* e[2][3];            /* [copy][Ex, Ey, Ez] */
+  void* h[2][3];            /* [copy][Hx, Hy, Hz] */
+  const void* ce;           /* [n_mat][nz][ny][pitch] */
+  const void* loss;
+} bz_fields3d;
+
+/* One 3D time step (H then E, E on the reference's interior slices) for every
+ * design and component; the launch reads copy (step & 1) and writes the other. */
+int bz_step3d(const bz_grid3d* g, const bz_fields3d* f, int64_t step, void* stream);
+
+/* Applies source operations (bz_source_ops, cell = (z*ny + y)*nx + x or y*nx + x)
+ * in place to one field array laid out [n_designs][n_comp][rows][pitch] with
+ * rows of nx cells, as helper.py:5-118 injects after the E update. The time index
+ * is step, or *d_step + step when d_step is non-NULL. */
+int bz_cell_ops(void* field, int32_t dtype, int32_t n_designs, int32_t n_comp, int64_t comp_stride,
+                int32_t nx, int32_t pitch, const bz_source_ops* ops, int64_t step, const int64_t* d_step,
+                void* stream);
+
+/* Gathers monitor samples: n_q quantities (<= 6) per point from arrays laid out
+ * [n_designs][n_comp][...] (element strides comp_stride between components),
+ * offset[p][q] into each quantity's array (-1: the sample is 0). Writes
+ * record[step - rec_step0][d][c][p][q] when in range and ring[step % ring_len][d][c][p][q]
+ * (either may be NULL). Reference: helper.py:235-244 -> monitors.py:317-396. */
+typedef struct bz_gather_ops {
+  int32_t n_points, n_q;
+  const void* src[6];
+  const int64_t* offset;
+  void* record;
+  int64_t rec_step0;
+  int32_t n_rec;
+  int32_t ring_len;
+  void* ring;
+} bz_gather_ops;
+int bz_gather(const bz_gather_ops* ops, int32_t dtype, int32_t n_designs, int32_t n_comp, int64_t comp_stride,
+              int64_t step, const int64_t* d_step, void* stream);
+
+/* Adds, per cell of the common region (nz-1, ny-1, nx-1), |Re(E x conj(H))| of
+ * fields copy `cur` to power[n_designs][nz-1][ny-1][nx-1] (float64), as
+ * helper.py:124-151 accumulates it. */
+int bz_power3d(const bz_grid3d* g, const bz_fields3d* f, int32_t cur, double* power, void* stream);
+
+/* bz_dft_fold with n_q quantities per item (<= 6), the first n_e on the E phasor and
+ * the rest on the H phasor; ring [ring_len][n_items][n_q], dft [n_items][n_freq][n_q][2]. */
+int bz_dft_fold_q(const void* ring, int32_t dtype, int32_t ring_len, int64_t n_items, int32_t n_q, int32_t n_e,
+                  int32_t n_freq, const double* phasor, int64_t n_phasor, int64_t step0, int32_t count, double* dft,
+                  void* stream);
+
+/* ----------------------------------------------------------------------------
  * Rasteriser (meshing.py:92-536): painter's-order supersampled blend of each
  * structure's material, then the additive PML conductivity pass.
  * ------------------------------------------------------------------------- */
@@ -236,6 +302,29 @@ int bz_rasterize2d(int32_t nx, int32_t ny, const double* xc, const double* yc,
                    const bz_pml2d* pmls, int32_t n_pml, const double* pml_table,
                    double dx, double eps0, double mu0,
                    double* eps, double* mu, double* sigma, void* stream);
+
+/* 3D rasteriser (meshing.py:616-781): for every cell (k, i, j) and every structure
+ * in painter's order whose layer range [k0, k1) holds k, count the cell's 9 xy
+ * samples inside the structure's polygon, weight by zw[k - k0] of the n_zs z samples
+ * (the reference ignores z, so zw = n_zs on its layers; the extrusion mode counts
+ * the z samples inside the structure's thickness), and blend with factor
+ * count*zw / (9*n_zs). Then add the PML: the 2D boundary tables of bz_rasterize2d
+ * applied to every layer with that cell's eps, plus an optional per-layer z-face
+ * term prof_z[k] = (profile, frequency factor) (profile < 0: none) with
+ * sigma_factor_z. Outputs [nz][ny][nx] float64. */
+typedef struct bz_shape3d {
+  int32_t i0, i1, j0, j1, k0, k1;
+  int32_t path0, npath;
+  int32_t zw_off;                /* offset into zw (one entry per layer of [k0, k1)) */
+  int32_t reserved;
+  double perm, permb, cond;
+} bz_shape3d;
+
+int bz_rasterize3d(int32_t nx, int32_t ny, int32_t nz, int32_t n_zs, const double* xc, const double* yc,
+                   const double* offs, const double* bg, const bz_shape3d* shapes, int32_t n_shapes,
+                   const int32_t* zw, const int32_t* paths, const double* verts, const bz_pml2d* pmls,
+                   int32_t n_pml, const double* pml_table, const double* prof_z, double sigma_factor_z, double dx,
+                   double eps0, double mu0, double* eps, double* mu, double* sigma, void* stream);
 
 #ifdef __cplusplus
 }

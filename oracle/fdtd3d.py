@@ -136,7 +136,10 @@ def plane_slices(mon, dx, dy, dz, F):
     return mon.plane_slices_3d(dx, dy, dz, {k: F[k].shape for k in F})
 
 
-def run(eps_r, sigma, dx, dy, dz, dt, n_steps, sources=(), monitors=(), accumulate_power=False, fields=None):
+def run(eps_r, sigma, dx, dy, dz, dt, n_steps, sources=(), monitors=(), accumulate_power=False, fields=None,
+        dft_freqs=None):
+    """Run n_steps; ``dft_freqs`` additionally accumulates, per monitor, the DFT of the
+    real part of the six plane samples (E at (n+1)dt, H at (n+1/2)dt), times dt."""
     nz, ny, nx = eps_r.shape
     F = zeros_fields(nz, ny, nx) if fields is None else {k: np.array(v) for k, v in fields.items()}
     keys = ("Ex", "Ey", "Ez", "Hx", "Hy", "Hz")
@@ -144,6 +147,8 @@ def run(eps_r, sigma, dx, dy, dz, dt, n_steps, sources=(), monitors=(), accumula
             for m in monitors]
     power = None
     inj = make_injectors(sources, dx, dy, dz, (nz, ny, nx))
+    freqs = None if dft_freqs is None else np.asarray(dft_freqs, dtype=float)
+    dft = [None] * len(mons)
     t = 0
     for n in range(n_steps):
         update(F, eps_r, sigma, dx, dy, dz, dt)
@@ -160,6 +165,15 @@ def run(eps_r, sigma, dx, dy, dz, dt, n_steps, sources=(), monitors=(), accumula
                 md["power"].append(np.sum(np.sqrt(sx ** 2 + sy ** 2 + sz ** 2)))
                 md["t"].append(t)
                 md["last"] = n
+        if freqs is not None:
+            w = 2 * np.pi * freqs
+            pe, ph = np.exp(-1j * w * ((n + 1.0) * dt)), np.exp(-1j * w * ((n + 0.5) * dt))
+            for i, md in enumerate(mons):
+                sl = plane_slices(md["m"], dx, dy, dz, F)
+                parts = np.stack([np.real(F[c][s]) for c, s in zip(keys, sl)], axis=-1)  # (n0, n1, 6)
+                phase = np.stack([pe] * 3 + [ph] * 3, axis=-1)  # (nf, 6)
+                term = parts[None] * phase[:, None, None, :]
+                dft[i] = term if dft[i] is None else dft[i] + term
         if accumulate_power:
             mz = min(F[c].shape[0] for c in keys)
             my = min(F[c].shape[1] for c in keys)
@@ -173,4 +187,6 @@ def run(eps_r, sigma, dx, dy, dz, dt, n_steps, sources=(), monitors=(), accumula
         t += dt
     recs = [dict(fields={c: np.array(md["rec"][c]) for c in keys}, power=np.asarray(md["power"]),
                  t=np.asarray(md["t"], dtype=float)) for md in mons]
-    return dict(fields=F, power=power, records=recs)
+    if freqs is not None:
+        dft = [None if d is None else d * dt for d in dft]
+    return dict(fields=F, power=power, records=recs, dft=dft)
