@@ -48,12 +48,19 @@ class Fields2D(C.Structure):
 
 class SourceOps(C.Structure):
     _fields_ = [("n_ops", i32), ("n_steps", i32), ("row_ptr", vp), ("cell", vp), ("mul", vp), ("weight", vp),
-                ("sig", vp), ("signals", vp)]
+                ("sig", vp), ("signals", vp), ("weight_stride", i64)]
 
 
 class MonitorOps(C.Structure):
     _fields_ = [("n_points", i32), ("ring_len", i32), ("row_ptr", vp), ("cell", vp), ("point", vp), ("record", vp),
-                ("rec_step0", i64), ("n_rec", i32), ("reserved", i32), ("ring", vp)]
+                ("rec_step0", i64), ("n_rec", i32), ("reserved", i32), ("ring", vp), ("region", vp), ("rx0", i32),
+                ("ry0", i32), ("rw", i32), ("rh", i32), ("reg_step0", i64), ("n_reg", i32), ("reserved2", i32)]
+
+
+class Adjoint2D(C.Structure):
+    _fields_ = [("e", vp * 2), ("hx", vp * 2), ("hy", vp * 2), ("ce", vp), ("loss", vp), ("grad", vp),
+                ("eps_region", vp), ("fwd_region", vp), ("rx0", i32), ("ry0", i32), ("rw", i32), ("rh", i32),
+                ("fwd_step0", i64), ("n_fwd", i32), ("reserved", i32)]
 
 
 class Grid3D(C.Structure):
@@ -110,6 +117,8 @@ _power3d = _sig("bz_power3d", C.c_int, [C.POINTER(Grid3D), C.POINTER(Fields3D), 
 _dft_fold_q = _sig("bz_dft_fold_q", C.c_int, [vp, i32, i32, i64, i32, i32, i32, vp, i64, i64, i32, vp, vp])
 _raster3d = _sig("bz_rasterize3d", C.c_int, [i32, i32, i32, i32, vp, vp, vp, vp, vp, i32, vp, vp, vp, vp, i32, vp,
                                               vp, f64, f64, f64, f64, vp, vp, vp, vp])
+_adjoint2d = _sig("bz_adjoint_step2d", C.c_int, [C.POINTER(Grid2D), C.POINTER(Adjoint2D), C.POINTER(SourceOps), i64,
+                                                  i32, vp])
 _advance = _sig("bz_advance_step", C.c_int, [vp, i64, vp])
 _prepare = _sig("bz_prepare_coeffs", C.c_int, [vp, vp, i64, i32, i32, i32, f64, f64, f64, vp, vp, vp])
 _upd_h2d = _sig("bz_update_h2d", C.c_int, [i32, i32, i32, i32, vp, vp, vp, vp, f64, f64, f64, f64, f64, vp])
@@ -119,7 +128,7 @@ _raster2d = _sig("bz_rasterize2d", C.c_int, [i32, i32, vp, vp, vp, vp, vp, vp, i
 
 #: every symbol include/beamz_b200.h declares (checked by the CPU test suite)
 EXPORTED = ["bz_version", "bz_last_error", "bz_step2d", "bz_dft_fold", "bz_step2d_dft_static", "bz_advance_step",
-            "bz_step3d", "bz_cell_ops", "bz_gather", "bz_power3d", "bz_dft_fold_q", "bz_rasterize3d", "bz_prepare_coeffs", "bz_update_h2d",
+            "bz_adjoint_step2d", "bz_step3d", "bz_cell_ops", "bz_gather", "bz_power3d", "bz_dft_fold_q", "bz_rasterize3d", "bz_prepare_coeffs", "bz_update_h2d",
             "bz_update_e2d", "bz_rasterize2d"]
 
 
@@ -196,3 +205,7 @@ def dft_fold_q(*args) -> None:
 
 def rasterize3d(*args) -> None:
     check(_raster3d(*args))
+
+
+def adjoint_step2d(grid, state, ops, step, phase, stream) -> None:
+    check(_adjoint2d(C.byref(grid), C.byref(state), C.byref(ops) if ops is not None else None, step, phase, stream))

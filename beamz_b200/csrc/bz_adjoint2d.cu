@@ -1,0 +1,253 @@
+// Exact discrete adjoint of the 2D step (bz_step2d), one time step backwards.
+//
+// Forward step n (coefficients per cell from ce, loss; interior mask I):
+//   Hx' = fh*Hx - cx*(E(x+1) - E(x))        Hy' = fh*Hy + cy*(E(y+1) - E(y))
+//   Et  = Fe*E + Ce*((Hx'(x-1) - Hx'(x)) - qy*(Hy'(y-1) - Hy'(y)))    Fe = I?fe:1, Ce = I?ce:0
+//   E_{n+1} = mul*Et + sources,   J reads E_{n+1} at monitor cells.
+// Reverse mode with e = dJ/dEt (already multiplied by mul and fed the objective's
+// dJ/dE_{n+1}), and carried adjoints hx, hy of H' from later steps:
+//   U   = Ce*e
+//   hx' = hx + U(x+1) - U(x)                hy' = hy - qy*(U(y+1) - U(y))
+//   wx  = cx*hx',  wy = cy*hy'   (zero where Hx, Hy do not exist)
+//   dJ/dE_n = Fe*e - (wx(x-1) - wx(x)) + (wy(y-1) - wy(y))
+//   carried: hx <- fh*hx', hy <- fh*hy'
+// The data flow mirrors the forward kernel (an H-like pass reading +1 neighbours,
+// then an E-like pass reading -1 neighbours), so the same column-march layout is
+// used. In the design region (no conductivity) dEt/d eps_r = -(Et - E_n)/eps_r, and
+// the kernel accumulates grad += -e*(E_{n+1} - E_n)/eps_r from captured forward
+// fields. The post phase then prepares the input of step n-1:
+//   e_{n-1} = mul*(dJ/dE_n + objective term), through the same source operations.
+#include "bz_stencil.cuh"
+
+namespace bz {
+namespace {
+
+constexpr int BX = 128;
+constexpr int RB = 16;
+constexpr unsigned FULL = 0xffffffffu;
+
+template <typename T>
+struct AdjArgs {
+  const T* e_in;
+  const T* hx_in;
+  const T* hy_in;
+  T* e_out;
+  T* hx_out;
+  T* hy_out;
+  const T* ce;
+  const T* loss;
+  int nx, ny, pitch, n_designs, n_mat;
+  long long plane;
+  T chx, chy, qy, inv_kd2;
+  // gradient
+  double* grad;
+  const double* eps_region;
+  const T* fwd;
+  int rx0, ry0, rw, rh, n_fwd;
+  long long fwd_step0;
+  // operations preparing step n-1
+  int n_src, src_steps;
+  const int* src_row;
+  const int* src_cell;
+  const T* src_mul;
+  const T* src_w;
+  long long w_stride;
+  const int* src_sig;
+  const T* signals;
+};
+
+template <typename T>
+__device__ __forceinline__ void cell_coeffs(const AdjArgs<T>& a, const T* lsp, const T* cep, long long r, int x,
+                                            int y, T& fh, T& cx, T& cy, T& Fe, T& Ce) {
+  const T ls = __ldg(lsp + r), c = __ldg(cep + r);
+  h_coeffs(ls, a.chx, a.chy, fh, cx, cy);
+  const bool interior = x >= 1 && x <= a.nx - 2 && y >= 1 && y <= a.ny - 2;
+  Fe = interior ? T(1) - ls * c * a.inv_kd2 : T(1);
+  Ce = interior ? c : T(0);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(BX) adjoint2d_kernel(AdjArgs<T> a, long long step) {
+  const int nx = a.nx, ny = a.ny, pitch = a.pitch;
+  const int x = blockIdx.x * BX + threadIdx.x;
+  const int wl = threadIdx.x & 31;
+  const int d = blockIdx.z;
+  const int y0 = blockIdx.y * RB;
+  const int nrows = min(RB, ny - y0);
+  const bool xin = x < nx;
+  const long long fb = (long long)d * a.plane;
+  const long long mb = (a.n_mat > 1 ? (long long)d : 0LL) * a.plane;
+  const T* lsp = a.loss + mb;
+  const T* cep = a.ce + mb;
+  const T* E = a.e_in + fb;
+
+  // U(y0, x) and the carried wy(y0-1, x) of the row above the tile
+  T fh, cx, cy, Fe, Ce;
+  T Uc = T(0), wy_up = T(0);
+  if (xin) {
+    cell_coeffs(a, lsp, cep, (long long)y0 * pitch + x, x, y0, fh, cx, cy, Fe, Ce);
+    Uc = Ce * __ldg(E + (long long)y0 * pitch + x);
+    if (y0 >= 1) {
+      const long long r = (long long)(y0 - 1) * pitch + x;
+      T fhm, cxm, cym, Fem, Cem;
+      cell_coeffs(a, lsp, cep, r, x, y0 - 1, fhm, cxm, cym, Fem, Cem);
+      const T Um = Cem * __ldg(E + r);
+      const T hyp = __ldg(a.hy_in + fb + r) - a.qy * (Uc - Um);
+      wy_up = cym * hyp;
+    }
+  }
+  for (int i = 0; i < RB; ++i) {
+    const int y = y0 + i;
+    if (i >= nrows) break;  // uniform across the block
+    const long long r = (long long)y * pitch + x;
+    T e = T(0);
+    if (xin) {
+      cell_coeffs(a, lsp, cep, r, x, y, fh, cx, cy, Fe, Ce);
+      e = __ldg(E + r);
+    }
+    T Un = T(0);  // U(y+1, x)
+    if (xin && y + 1 < ny) {
+      T fh1, cx1, cy1, Fe1, Ce1;
+      cell_coeffs(a, lsp, cep, r + pitch, x, y + 1, fh1, cx1, cy1, Fe1, Ce1);
+      Un = Ce1 * __ldg(E + r + pitch);
+    }
+    T Ur = __shfl_down_sync(FULL, Uc, 1);  // U(y, x+1)
+    if (wl == 31) {
+      Ur = T(0);
+      if (x + 1 < nx) {
+        T f1, c1, c2, Fe1, Ce1;
+        cell_coeffs(a, lsp, cep, r + 1, x + 1, y, f1, c1, c2, Fe1, Ce1);
+        Ur = Ce1 * __ldg(E + r + 1);
+      }
+    }
+    const T hx0 = xin ? __ldg(a.hx_in + fb + r) : T(0);
+    const T hy0 = xin ? __ldg(a.hy_in + fb + r) : T(0);
+    const T hxp = hx0 + (Ur - Uc);
+    const T hyp = hy0 - a.qy * (Un - Uc);
+    const T wx = (x < nx - 1) ? cx * hxp : T(0);
+    const T wy = (y < ny - 1) ? cy * hyp : T(0);
+    T wx_left = __shfl_up_sync(FULL, wx, 1);
+    if (wl == 0) {
+      wx_left = T(0);
+      if (xin && x >= 1) {  // recompute wx(y, x-1) of the lane to the left
+        T fl, cxl, cyl, Fel, Cel;
+        cell_coeffs(a, lsp, cep, r - 1, x - 1, y, fl, cxl, cyl, Fel, Cel);
+        const T Ul = Cel * __ldg(E + r - 1);
+        wx_left = cxl * (__ldg(a.hx_in + fb + r - 1) + (Uc - Ul));
+      }
+    }
+    if (xin) {
+      const T e_prev = Fe * e - (wx_left - wx) + (wy_up - wy);
+      a.e_out[fb + r] = e_prev;
+      if (x < nx - 1) a.hx_out[fb + r] = fh * hxp;
+      if (y < ny - 1) a.hy_out[fb + r] = fh * hyp;
+      if (a.grad != nullptr) {
+        const int rx = x - a.rx0, ry = y - a.ry0;
+        const long long s1 = step + 1 - a.fwd_step0;
+        if (rx >= 0 && rx < a.rw && ry >= 0 && ry < a.rh && s1 >= 1 && s1 < a.n_fwd) {
+          const long long cell = (long long)ry * a.rw + rx;
+          const long long per = (long long)a.n_designs * a.rh * a.rw;
+          const double en1 = (double)a.fwd[s1 * per + (long long)d * a.rh * a.rw + cell];
+          const double en0 = (double)a.fwd[(s1 - 1) * per + (long long)d * a.rh * a.rw + cell];
+          const double er = a.eps_region[(a.n_mat > 1 ? (long long)d : 0LL) * a.rh * a.rw + cell];
+          a.grad[(long long)d * a.rh * a.rw + cell] -= (double)e * (en1 - en0) / er;
+        }
+      }
+    }
+    Uc = Un;
+    wy_up = wy;
+  }
+
+  if (a.n_src == 0 || step == 0) return;
+  // ---- post phase: e_{n-1} = mul * (dJ/dE_n + objective term at step n-1) ---------
+  __shared__ int s_k0[RB], s_pre[RB + 1];
+  const int xlo = blockIdx.x * BX;
+  const int xhi = min(xlo + BX, nx);
+  __syncthreads();
+  const int total = block_op_ranges(a.src_row, a.src_cell, y0, nrows, nx, xlo, xhi, s_k0, s_pre);
+  const long long sstep = step - 1;
+  for (int i = threadIdx.x; i < total; i += BX) {
+    int t;
+    const int k = op_at(i, nrows, s_k0, s_pre, t);
+    const int cell = __ldg(a.src_cell + k);
+    if (i > s_pre[t] && __ldg(a.src_cell + k - 1) == cell) continue;
+    const int y = y0 + t;
+    const long long rr = fb + (long long)y * pitch + (cell - y * nx);
+    T v = a.e_out[rr];
+    for (int kk = k; kk < a.n_src && __ldg(a.src_cell + kk) == cell; ++kk) {
+      const T s = sstep < a.src_steps ? __ldg(a.signals + (long long)__ldg(a.src_sig + kk) * a.src_steps + sstep) : T(0);
+      v = __ldg(a.src_mul + kk) * v + __ldg(a.src_w + d * a.w_stride + kk) * s;
+    }
+    a.e_out[rr] = v;
+  }
+}
+
+template <typename T>
+int launch_adj(const bz_grid2d* g, const bz_adjoint2d* s, const bz_source_ops* ops, int64_t step, int32_t phase,
+               cudaStream_t st) {
+  AdjArgs<T> a = {};
+  const int src = phase & 1;
+  a.e_in = (const T*)s->e[src];
+  a.hx_in = (const T*)s->hx[src];
+  a.hy_in = (const T*)s->hy[src];
+  a.e_out = (T*)s->e[src ^ 1];
+  a.hx_out = (T*)s->hx[src ^ 1];
+  a.hy_out = (T*)s->hy[src ^ 1];
+  a.ce = (const T*)s->ce;
+  a.loss = (const T*)s->loss;
+  a.nx = g->nx;
+  a.ny = g->ny;
+  a.pitch = g->pitch;
+  a.n_designs = g->n_designs;
+  a.n_mat = g->n_mat;
+  a.plane = (long long)g->ny * g->pitch;
+  a.chx = (T)g->chx;
+  a.chy = (T)g->chy;
+  a.qy = (T)g->qy;
+  a.inv_kd2 = (T)g->inv_kd2;
+  a.grad = s->grad;
+  a.eps_region = s->eps_region;
+  a.fwd = (const T*)s->fwd_region;
+  a.rx0 = s->rx0;
+  a.ry0 = s->ry0;
+  a.rw = s->rw;
+  a.rh = s->rh;
+  a.n_fwd = s->n_fwd;
+  a.fwd_step0 = s->fwd_step0;
+  if (ops && ops->n_ops > 0) {
+    a.n_src = ops->n_ops;
+    a.src_steps = ops->n_steps;
+    a.src_row = ops->row_ptr;
+    a.src_cell = ops->cell;
+    a.src_mul = (const T*)ops->mul;
+    a.src_w = (const T*)ops->weight;
+    a.w_stride = ops->weight_stride;
+    a.src_sig = ops->sig;
+    a.signals = (const T*)ops->signals;
+  }
+  dim3 grid((unsigned)ceil_div(g->nx, BX), (unsigned)ceil_div(g->ny, RB), (unsigned)g->n_designs);
+  adjoint2d_kernel<T><<<grid, BX, 0, st>>>(a, (long long)step);
+  return check_launch("bz_adjoint_step2d");
+}
+
+}  // namespace
+}  // namespace bz
+
+extern "C" int bz_adjoint_step2d(const bz_grid2d* g, const bz_adjoint2d* s, const bz_source_ops* ops, int64_t step,
+                                 int32_t phase, void* stream) {
+  BZ_REQUIRE(g && s, "bz_adjoint_step2d: grid or state is NULL");
+  BZ_REQUIRE(g->n_comp == 1, "bz_adjoint_step2d: only real fields (n_comp = 1)");
+  BZ_REQUIRE(g->nx >= 2 && g->ny >= 2 && g->pitch >= g->nx && g->pitch % 32 == 0, "bz_adjoint_step2d: bad grid");
+  BZ_REQUIRE(g->n_mat == 1 || g->n_mat == g->n_designs, "bz_adjoint_step2d: n_mat must be 1 or n_designs");
+  for (int i = 0; i < 2; ++i) BZ_REQUIRE(s->e[i] && s->hx[i] && s->hy[i], "bz_adjoint_step2d: NULL state buffer");
+  BZ_REQUIRE(s->ce && s->loss, "bz_adjoint_step2d: NULL coefficients");
+  if (s->grad) BZ_REQUIRE(s->eps_region && s->fwd_region && s->rw >= 1 && s->rh >= 1, "bz_adjoint_step2d: bad grad box");
+  if (ops && ops->n_ops > 0)
+    BZ_REQUIRE(ops->row_ptr && ops->cell && ops->mul && ops->weight && ops->sig && ops->signals,
+               "bz_adjoint_step2d: incomplete ops");
+  BZ_REQUIRE(step >= 0, "bz_adjoint_step2d: negative step");
+  cudaStream_t st = bz::as_stream(stream);
+  if (g->dtype == BZ_F32) return bz::launch_adj<float>(g, s, ops, step, phase, st);
+  if (g->dtype == BZ_F64) return bz::launch_adj<double>(g, s, ops, step, phase, st);
+  return bz::fail(BZ_ERR_INVALID, "bz_adjoint_step2d: unknown dtype %d", g->dtype);
+}

@@ -19,7 +19,7 @@
 //
 // After the tile is written, the block applies the source and monitor
 // operations that fall inside it, spread over all its threads.
-#include "bz_internal.cuh"
+#include "bz_stencil.cuh"
 
 namespace bz {
 namespace {
@@ -41,6 +41,7 @@ struct Ops2D {
   const int* src_cell;
   const T* src_mul;
   const T* src_w;
+  long long w_stride;
   const int* src_sig;
   const T* signals;
   int n_mon, ring_len;
@@ -51,31 +52,10 @@ struct Ops2D {
   long long rec_step0;
   int n_rec;
   T* ring;
+  T* region;
+  int rx0, ry0, rw, rh, n_reg;
+  long long reg_step0;
 };
-
-// H-update factors for a cell with conductivity term a (numpy_backend.py:52-60):
-// factor = (1-a)/(1+a), source = c/(1+a). a == 0 (all non-PML cells) is exact.
-template <typename T>
-__device__ __forceinline__ void h_coeffs(T a, T chx, T chy, T& fh, T& cx, T& cy) {
-  if (a == T(0)) {
-    fh = T(1);
-    cx = chx;
-    cy = chy;
-  } else {
-    const T den = T(1) + a;
-    fh = (T(1) - a) / den;
-    cx = chx / den;
-    cy = chy / den;
-  }
-}
-
-__device__ __forceinline__ int lower_bound_i(const int* a, int lo, int hi, int key) {
-  while (lo < hi) {
-    const int mid = (lo + hi) >> 1;
-    if (__ldg(a + mid) < key) lo = mid + 1; else hi = mid;
-  }
-  return lo;
-}
 
 template <typename T>
 __device__ __forceinline__ double sq_pow(const T* ez, const T* hx, const T* hy, int nc) {
@@ -86,40 +66,6 @@ __device__ __forceinline__ double sq_pow(const T* ez, const T* hx, const T* hy, 
     sy += (double)ez[c] * (double)hx[c];
   }
   return sx * sx + sy * sy;
-}
-
-// Operation ranges of the block's rows: thread t < nrows finds, in row y0+t, the
-// sorted operations whose cell lies in [xlo, xhi); prefix sums let all threads
-// share the flattened list.
-template <int RB>
-__device__ __forceinline__ int block_op_ranges(const int* row_ptr, const int* cells, int y0, int nrows, int nx,
-                                               int xlo, int xhi, int* s_k0, int* s_pre) {
-  if (threadIdx.x < nrows) {
-    const int y = y0 + threadIdx.x;
-    const int lo = __ldg(row_ptr + y), hi = __ldg(row_ptr + y + 1);
-    int k0 = lo, k1 = lo;
-    if (lo < hi) {
-      k0 = lower_bound_i(cells, lo, hi, y * nx + xlo);
-      k1 = lower_bound_i(cells, k0, hi, y * nx + xhi);
-    }
-    s_k0[threadIdx.x] = k0;
-    s_pre[threadIdx.x + 1] = k1 - k0;
-  }
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    s_pre[0] = 0;
-    for (int t = 0; t < nrows; ++t) s_pre[t + 1] += s_pre[t];
-  }
-  __syncthreads();
-  return s_pre[nrows];
-}
-
-// k-th operation of the flattened block list -> (row offset t, op index).
-template <int RB>
-__device__ __forceinline__ int op_at(int i, int nrows, const int* s_k0, const int* s_pre, int& t) {
-  t = 0;
-  while (t + 1 < nrows && s_pre[t + 1] <= i) ++t;
-  return s_k0[t] + (i - s_pre[t]);
 }
 
 template <typename T, int NC, bool PWR, int RB>
@@ -207,20 +153,29 @@ __global__ void __launch_bounds__(BX) step2d_kernel(
         hyp[c] = hyn;
       }
       if (PWR && xin) pwr[(long long)d * g.plane + r] += sq_pow<T>(ezo, hxo, hyo, NC);
+      if (o.region != nullptr) {  // Ez after this step inside the capture box
+        const long long slot = step + 1 - o.reg_step0;
+        const int rx = x - o.rx0, ry = y - o.ry0;
+        if (slot >= 1 && slot < o.n_reg && rx >= 0 && rx < o.rw && ry >= 0 && ry < o.rh) {
+#pragma unroll
+          for (int c = 0; c < NC; ++c)
+            o.region[(((slot * g.n_designs + d) * NC + c) * o.rh + ry) * (long long)o.rw + rx] = ezo[c];
+        }
+      }
     }
   }
 
-  if (o.n_src == 0 && o.n_mon == 0) return;
+  if (o.n_src == 0 && o.n_mon == 0) return;  // uniform across the grid
   // ---- post phase: operations on cells of this block's tile -----------------
   __shared__ int s_k0[RB], s_pre[RB + 1];
   const int xlo = blockIdx.x * BX;
   const int xhi = min(xlo + BX, nx);
   __syncthreads();  // this block's field writes are now visible to all its threads
   if (o.n_src > 0) {
-    const int total = block_op_ranges<RB>(o.src_row, o.src_cell, y0, nrows, nx, xlo, xhi, s_k0, s_pre);
+    const int total = block_op_ranges(o.src_row, o.src_cell, y0, nrows, nx, xlo, xhi, s_k0, s_pre);
     for (int i = threadIdx.x; i < total; i += BX) {
       int t;
-      const int k = op_at<RB>(i, nrows, s_k0, s_pre, t);
+      const int k = op_at(i, nrows, s_k0, s_pre, t);
       const int cell = __ldg(o.src_cell + k);
       if (i > s_pre[t] && __ldg(o.src_cell + k - 1) == cell) continue;  // not first of its cell's run
       const int y = y0 + t;
@@ -239,7 +194,7 @@ __global__ void __launch_bounds__(BX) step2d_kernel(
         const int sg = __ldg(o.src_sig + kk);
         const T s = (step < o.src_steps) ? __ldg(o.signals + (long long)sg * o.src_steps + step) : T(0);
 #pragma unroll
-        for (int c = 0; c < NC; ++c) e[c] = m * e[c] + __ldg(o.src_w + (long long)kk * NC + c) * s;
+        for (int c = 0; c < NC; ++c) e[c] = m * e[c] + __ldg(o.src_w + d * o.w_stride + (long long)kk * NC + c) * s;
       }
 #pragma unroll
       for (int c = 0; c < NC; ++c) ez_out[fb + c * g.plane + rr] = e[c];
@@ -251,12 +206,12 @@ __global__ void __launch_bounds__(BX) step2d_kernel(
     __syncthreads();
   }
   if (o.n_mon > 0) {
-    const int total = block_op_ranges<RB>(o.mon_row, o.mon_cell, y0, nrows, nx, xlo, xhi, s_k0, s_pre);
+    const int total = block_op_ranges(o.mon_row, o.mon_cell, y0, nrows, nx, xlo, xhi, s_k0, s_pre);
     const bool rec = o.record != nullptr && step >= o.rec_step0 && step < o.rec_step0 + o.n_rec;
     const long long slot = o.ring != nullptr ? step % o.ring_len : 0;
     for (int i = threadIdx.x; i < total; i += BX) {
       int t;
-      const int k = op_at<RB>(i, nrows, s_k0, s_pre, t);
+      const int k = op_at(i, nrows, s_k0, s_pre, t);
       const int cell = __ldg(o.mon_cell + k);
       const int p = __ldg(o.mon_point + k);
       const int y = y0 + t;
@@ -309,6 +264,7 @@ int launch(const bz_grid2d* gd, const bz_fields2d* f, const bz_source_ops* s, co
     o.src_cell = s->cell;
     o.src_mul = (const T*)s->mul;
     o.src_w = (const T*)s->weight;
+    o.w_stride = s->weight_stride;
     o.src_sig = s->sig;
     o.signals = (const T*)s->signals;
   }
@@ -322,6 +278,15 @@ int launch(const bz_grid2d* gd, const bz_fields2d* f, const bz_source_ops* s, co
     o.rec_step0 = m->rec_step0;
     o.n_rec = m->n_rec;
     o.ring = (T*)m->ring;
+  }
+  if (m && m->region && m->n_reg > 1) {
+    o.region = (T*)m->region;
+    o.rx0 = m->rx0;
+    o.ry0 = m->ry0;
+    o.rw = m->rw;
+    o.rh = m->rh;
+    o.n_reg = m->n_reg;
+    o.reg_step0 = m->reg_step0;
   }
   const int src = (int)(step & 1);  // copy read by this launch: parity of the host-side step argument
   dim3 grid((unsigned)ceil_div(gd->nx, BX), (unsigned)ceil_div(gd->ny, RB), (unsigned)gd->n_designs);
@@ -373,6 +338,7 @@ extern "C" int bz_step2d(const bz_grid2d* g, const bz_fields2d* f, const bz_sour
   if (s && s->n_ops > 0)
     BZ_REQUIRE(s->row_ptr && s->cell && s->mul && s->weight && s->sig && s->signals && s->n_steps >= 0,
                "bz_step2d: incomplete source ops");
+  if (m && m->region) BZ_REQUIRE(m->rw >= 1 && m->rh >= 1 && m->n_reg >= 1, "bz_step2d: bad capture box");
   if (m && m->n_points > 0) {
     BZ_REQUIRE(m->row_ptr && m->cell && m->point, "bz_step2d: incomplete monitor ops");
     BZ_REQUIRE(m->ring == nullptr || m->ring_len >= 1, "bz_step2d: ring without length");

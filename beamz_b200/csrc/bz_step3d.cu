@@ -230,8 +230,9 @@ int dispatch3d(const bz_grid3d* g, const bz_fields3d* f, int64_t step, cudaStrea
 template <typename T>
 __global__ void cell_ops_kernel(T* __restrict__ field, int n_comp, long long comp_stride, int nx, int pitch,
                                 int n_ops, int n_steps, const int* __restrict__ cell, const T* __restrict__ mul,
-                                const T* __restrict__ w, const int* __restrict__ sig, const T* __restrict__ signals,
-                                long long step_base, const long long* __restrict__ d_step) {
+                                const T* __restrict__ w, long long w_stride, const int* __restrict__ sig,
+                                const T* __restrict__ signals, long long step_base,
+                                const long long* __restrict__ d_step) {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= n_ops) return;
   const int c0 = __ldg(cell + k);
@@ -244,7 +245,7 @@ __global__ void cell_ops_kernel(T* __restrict__ field, int n_comp, long long com
     T v = *p;
     for (int kk = k; kk < n_ops && __ldg(cell + kk) == c0; ++kk) {
       const T s = step < n_steps ? __ldg(signals + (long long)__ldg(sig + kk) * n_steps + step) : T(0);
-      v = __ldg(mul + kk) * v + __ldg(w + (long long)kk * n_comp + c) * s;
+      v = __ldg(mul + kk) * v + __ldg(w + d * w_stride + (long long)kk * n_comp + c) * s;
     }
     *p = v;
   }
@@ -333,12 +334,12 @@ extern "C" int bz_cell_ops(void* field, int32_t dtype, int32_t n_designs, int32_
   if (dtype == BZ_F32)
     bz::cell_ops_kernel<float><<<grid, 128, 0, st>>>((float*)field, n_comp, comp_stride, nx, pitch, ops->n_ops,
                                                      ops->n_steps, ops->cell, (const float*)ops->mul,
-                                                     (const float*)ops->weight, ops->sig,
+                                                     (const float*)ops->weight, ops->weight_stride, ops->sig,
                                                      (const float*)ops->signals, step, (const long long*)d_step);
   else if (dtype == BZ_F64)
     bz::cell_ops_kernel<double><<<grid, 128, 0, st>>>((double*)field, n_comp, comp_stride, nx, pitch, ops->n_ops,
                                                       ops->n_steps, ops->cell, (const double*)ops->mul,
-                                                      (const double*)ops->weight, ops->sig,
+                                                      (const double*)ops->weight, ops->weight_stride, ops->sig,
                                                       (const double*)ops->signals, step, (const long long*)d_step);
   else
     return bz::fail(BZ_ERR_INVALID, "bz_cell_ops: unknown dtype %d", dtype);

@@ -201,7 +201,9 @@ class Monitor:
     def plane_slices_3d(self, dx, dy, dz, shapes):
         """Per-component index tuples of the recorded plane (monitors.py:317-371):
         the plane slice clamped to each staggered array, then cropped to the common
-        overlap of all six components."""
+        overlap of all six components. z-normal planes follow the reference exactly;
+        for x- and y-normal planes the reference's slicing falls back to whole arrays
+        and fails, so here they are sliced the same way along their own axes."""
         si = self.get_grid_slice_3d(dx, dy, dz)
         out = []
         for k in ("Ex", "Ey", "Ez", "Hx", "Hy", "Hz"):
@@ -214,7 +216,7 @@ class Monitor:
                 xe = max(xs, min(si[1].stop or a2, a2))
                 out.append([zi, ys, ye, xs, xe, "z"])
             elif self.plane_normal == "y":
-                s0, s1, fixed = si
+                fixed, s1, s0 = si  # (y index, x slice, z slice)
                 fe = max(0, min(fixed, a1 - 1))
                 xs = max(0, min(s1.start or 0, a2 - 1))
                 xe = max(xs, min(s1.stop or a2, a2))
@@ -222,7 +224,7 @@ class Monitor:
                 ze = max(zs, min(s0.stop or a0, a0))
                 out.append([fe, zs, ze, xs, xe, "y"])
             else:
-                s0, s1, fixed = si
+                s0, fixed, s1 = si  # (y slice, x index, z slice)
                 fe = max(0, min(fixed, a2 - 1))
                 ys = max(0, min(s0.start or 0, a1 - 1))
                 ye = max(ys, min(s0.stop or a1, a1))

@@ -33,7 +33,7 @@ class Engine2D:
         eps_r = np.asarray(eps_r, dtype=np.float64)
         sigma = np.asarray(sigma, dtype=np.float64)
         if eps_r.ndim == 2:
-            eps_r, sigma = eps_r[None], sigma[None]
+            eps_r = eps_r[None]
         self.n_mat, self.ny, self.nx = eps_r.shape
         if self.nx < 2 or self.ny < 2:
             raise ValueError("2D grid must be at least 2 x 2 cells")
@@ -78,8 +78,11 @@ class Engine2D:
 
     # ---- set-up ---------------------------------------------------------------
     def set_material(self, eps_r, sigma):
-        eps_r = np.ascontiguousarray(np.asarray(eps_r, dtype=np.float64).reshape(self.n_mat, self.ny, self.nx))
-        sigma = np.ascontiguousarray(np.asarray(sigma, dtype=np.float64).reshape(self.n_mat, self.ny, self.nx))
+        """Uploads new material ([n_mat][ny][nx] or (ny, nx), sigma may be shared) and
+        recomputes the update coefficients."""
+        shape = (self.n_mat, self.ny, self.nx)
+        eps_r = np.ascontiguousarray(np.broadcast_to(np.asarray(eps_r, dtype=np.float64), shape))
+        sigma = np.ascontiguousarray(np.broadcast_to(np.asarray(sigma, dtype=np.float64), shape))
         te = torch.as_tensor(eps_r).to(self.dev)
         ts = torch.as_tensor(sigma).to(self.dev)
         self.h2d_bytes += eps_r.nbytes + sigma.nbytes

@@ -103,6 +103,7 @@ typedef struct bz_source_ops {
   const void* weight;       /* [n_ops][n_comp] dtype */
   const int32_t* sig;       /* [n_ops] signal row */
   const void* signals;      /* [n_signals][n_steps] dtype */
+  int64_t weight_stride;    /* elements between designs' weight tables; 0: one table for all designs */
 } bz_source_ops;
 
 /* Monitor sampling after injection (monitors.py:279-315). Each point samples,
@@ -125,6 +126,15 @@ typedef struct bz_monitor_ops {
   int32_t n_rec;
   int32_t reserved;
   void* ring;
+  /* optional capture of Ez inside a box (design region), for adjoint gradients:
+   * region[k][d][c][rh][rw] = Ez after step (reg_step0 + k - 1) for 1 <= k < n_reg
+   * (slot 0 is left to the caller, which stores the state at reg_step0); the box must
+   * not contain source cells */
+  void* region;
+  int32_t rx0, ry0, rw, rh;
+  int64_t reg_step0;
+  int32_t n_reg;
+  int32_t reserved2;
 } bz_monitor_ops;
 
 /* One full time step of the 2D Ez-mode Yee scheme for every design and component:
@@ -162,6 +172,37 @@ int bz_dft_fold(const void* ring, int32_t dtype, int32_t ring_len, int64_t n_ite
 int bz_step2d_dft_static(const bz_grid2d* g, const bz_fields2d* f, const bz_source_ops* src,
                          const bz_monitor_ops* mon, int64_t step0, int32_t n_steps, int32_t n_freq,
                          const double* phasor, int64_t n_phasor, double* dft, void* stream);
+
+/* Exact discrete adjoint of one 2D step (reverse-mode derivative of bz_step2d), for
+ * topology-optimisation gradients. No counterpart in the reference, whose adjoint
+ * (examples/4_topo.py:333-341) is a field-overlap heuristic; this one is the
+ * transpose of the update, so gradients match finite differences.
+ * State (n_comp = 1): e = dJ/dE (after the source zeroing), hx, hy = dJ/dH carried
+ * from later steps; two copies each, the launch reads copy (phase & 1) and writes
+ * the other. Step `step` = n maps the adjoint of E after step n to that of E_n.
+ * Gradient (optional): grad[d][rh][rw] += -e * (E_{n+1} - E_n) / eps_r over the box
+ * (rx0, ry0, rw, rh), reading forward captures fwd_region[k][d][rh][rw] = E at step
+ * fwd_step0 + k (k < n_fwd) and eps_region[n_mat][rh][rw] (float64); the box must be
+ * free of conductivity and sources. ops (optional): per-cell operations
+ * v = mul*v + weight*signal[step-1] applied to the output to prepare step n-1 (the
+ * source zeroing mask and the objective's dJ/dE_n, weights pre-multiplied by mul). */
+typedef struct bz_adjoint2d {
+  void* e[2];
+  void* hx[2];
+  void* hy[2];
+  const void* ce;
+  const void* loss;
+  double* grad;
+  const double* eps_region;
+  const void* fwd_region;
+  int32_t rx0, ry0, rw, rh;
+  int64_t fwd_step0;
+  int32_t n_fwd;
+  int32_t reserved;
+} bz_adjoint2d;
+
+int bz_adjoint_step2d(const bz_grid2d* g, const bz_adjoint2d* s, const bz_source_ops* ops, int64_t step,
+                      int32_t phase, void* stream);
 
 /* Adds n to the device step counter (*d_step += n). */
 int bz_advance_step(int64_t* d_step, int64_t n, void* stream);

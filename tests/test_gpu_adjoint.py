@@ -1,0 +1,90 @@
+"""Adjoint gradients of the batched 2D objective (mode power at one frequency on a
+line monitor) against central finite differences of the same GPU simulation and
+the objective itself against the float64 oracle.
+Tolerances: fp64 gradient vs central differences rtol 1e-5 (h = 1e-3 in eps_r);
+fp32 gradient vs the fp64 adjoint rtol 2e-3; objective vs oracle 1e-10."""
+import numpy as np
+import pytest
+
+from oracle import fdtd2d
+
+pytestmark = pytest.mark.gpu
+
+
+def _problem(bz, B=1, precision="fp64", n_steps=360, K=128, seed=0):
+    from beamz_b200.optimization.adjoint import AdjointFDTD2D
+
+    ny, nx, dx = 48, 64, 20e-9
+    eps = np.full((ny, nx), 2.085)
+    eps[20:28, :] = 12.25
+    sigma = np.zeros((ny, nx))
+    for k in range(6):
+        v = 3e5 * ((6 - k) / 6) ** 3
+        sigma[:, k] += v; sigma[:, nx - 1 - k] += v; sigma[k, :] += v; sigma[ny - 1 - k, :] += v  # noqa: E702
+    dt = 0.99 * dx / (bz.LIGHT_SPEED * np.sqrt(2))
+    t = np.arange(n_steps) * dt
+    f0 = bz.LIGHT_SPEED / 1.55e-6
+    sig = np.sin(2 * np.pi * f0 * t) * np.exp(-((t - 80 * dt) / (30 * dt)) ** 2)
+    src = bz.GaussianSource(position=(10 * dx, 24 * dx), width=dx / 10, signal=sig)
+    mon = bz.Monitor(start=(52 * dx, 14 * dx), end=(52 * dx, 34 * dx))
+    npts = 21
+    y = np.arange(npts) - 10
+    mode = np.exp(-(y / 4.0) ** 2).astype(complex)
+    region = (16, 24, 16, 14)
+    prob = AdjointFDTD2D(eps, sigma, dx, dt, n_steps, [src], mon, mode, f0, region, n_designs=B,
+                         precision=precision, checkpoint_every=K)
+    rng = np.random.default_rng(seed)
+    er = 2.085 + 10.165 * rng.random((B, region[2], region[3]))
+    return prob, er, eps, sigma, dx, dt, n_steps, src, mon, mode, f0, region
+
+
+def test_adjoint_matches_central_differences_fp64(bz):
+    prob, er, *_ = _problem(bz)
+    J, g = prob.value_and_grad(er)
+    rng = np.random.default_rng(99)
+    h = 1e-3
+    for _ in range(8):
+        i, j = rng.integers(0, er.shape[1]), rng.integers(0, er.shape[2])
+        ep, em = er.copy(), er.copy()
+        ep[0, i, j] += h
+        em[0, i, j] -= h
+        fd = (prob.forward(ep, keep_checkpoints=False)[0] - prob.forward(em, keep_checkpoints=False)[0]) / (2 * h)
+        assert abs(fd - g[0, i, j]) <= 1e-5 * max(abs(fd), 1e-3 * np.abs(g).max()), (i, j, fd, g[0, i, j])
+    assert np.abs(g).max() > 0 and J[0] > 0
+
+
+def test_objective_matches_oracle(bz):
+    prob, er, eps, sigma, dx, dt, n_steps, src, mon, mode, f0, region = _problem(bz)
+    J = prob.forward(er)
+    y0, x0, h, w = region
+    e = eps.copy()
+    e[y0:y0 + h, x0:x0 + w] = er[0]
+    ref = fdtd2d.run(e, sigma, dx, dx, dt, n_steps, [src], [mon], complex_fields=False, dft_freqs=[f0], record=False)
+    a = ref["dft"][0][0, :, 0] @ (np.conj(mode) * dx)
+    assert abs(J[0] - abs(a) ** 2) <= 1e-10 * abs(a) ** 2
+
+
+def test_adjoint_fp32_close_to_fp64_and_batch_independent(bz):
+    prob64, er, *_ = _problem(bz, B=3, precision="fp64", seed=3)
+    J64, g64 = prob64.value_and_grad(er)
+    prob32, *_ = _problem(bz, B=3, precision="fp32", seed=3)
+    J32, g32 = prob32.value_and_grad(er)
+    np.testing.assert_allclose(J32, J64, rtol=2e-4)
+    for b in range(3):
+        assert np.linalg.norm(g32[b] - g64[b]) <= 2e-3 * np.linalg.norm(g64[b])
+    single, *_ = _problem(bz, B=1, precision="fp64", seed=3)
+    J1, g1 = single.value_and_grad(er[1:2])
+    np.testing.assert_allclose(g1[0], g64[1], rtol=1e-9, atol=1e-12 * np.abs(g64[1]).max())
+
+
+def test_autograd_function(bz):
+    import torch
+
+    from beamz_b200.optimization.adjoint import FDTDObjective
+
+    prob, er, *_ = _problem(bz, B=2)
+    x = torch.tensor(er, dtype=torch.float64, requires_grad=True)
+    J = FDTDObjective.apply(x, prob)
+    (J * torch.tensor([1.0, -2.0], dtype=torch.float64)).sum().backward()
+    _, g = prob.value_and_grad(er)
+    np.testing.assert_allclose(x.grad.numpy(), g * np.array([1.0, -2.0])[:, None, None], rtol=1e-12)
