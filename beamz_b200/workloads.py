@@ -117,3 +117,46 @@ def soi_mmi_3d(nx=600, ny=300, nz=150, dx=0.02 * µm, n_steps=8000, pml=16, grid
                      plane_position=x_out, size=(1.2 * µm, 1.0 * µm), name=name, wavelengths=MMI_WAVELENGTHS,
                      record_fields=False, accumulate_power=False)
     return d, t, dx
+
+
+def topo_2d(n_designs=64, nx=600, ny=400, dx=0.02 * µm, n_steps=8000, pml=20, region_cells=120, seed=1234,
+            mode_points=None):
+    """Batched topology-optimisation problem: B densities (120x120 cells, uniform in
+    [0, 1] then Gaussian-smoothed with sigma = 3 cells, seeds seed+b) mapped to
+    eps = 2.085 + rho * (12.25 - 2.085), centred in a 600x400 grid between 500 nm input
+    and output Si waveguides in SiO2; CW mode source at 1.55 um; the objective is the
+    power in the output guide's fundamental slab mode at 1.55 um (monitor line 1 um
+    before the right PML). Returns a dict of AdjointFDTD2D arguments plus rho0 and the
+    material mapping."""
+    from scipy.ndimage import gaussian_filter
+
+    from .devices.mode import slab_mode_source
+    from .simulation.meshing import RegularGrid
+
+    W, H = (nx + 0.5) * dx, (ny + 0.5) * dx
+    d = _grade(Design(width=W, height=H, material=Material(2.085), pml_size=pml * dx), pml)
+    yc = H / 2
+    wg = 0.5 * µm
+    r = region_cells
+    y0, x0 = ny // 2 - r // 2, nx // 2 - r // 2
+    d += Rectangle(position=(0, yc - wg / 2), width=x0 * dx, height=wg, material=Material(12.25))
+    d += Rectangle(position=((x0 + r) * dx, yc - wg / 2), width=W - (x0 + r) * dx, height=wg,
+                   material=Material(12.25))
+    t = np.arange(n_steps) * courant_dt(dx)
+    f0 = LIGHT_SPEED / (1.55 * µm)
+    sig = ramped_cosine(t, amplitude=1.0, frequency=f0, phase=0, ramp_duration=20 / f0, t_max=t[-1] * 2)
+    src = ModeSource(design=d, position=(pml * dx + 0.6 * µm, yc), width=2.0 * µm, wavelength=1.55 * µm, signal=sig,
+                     direction="+x", num_modes=1)
+    grid = RegularGrid(d, dx)
+    x_mon = (nx - pml - 50) * dx
+    mon = Monitor(start=(x_mon, yc - 1.0 * µm), end=(x_mon, yc + 1.0 * µm))
+    pts = mon.get_grid_points_2d(dx, dx)
+    ys = np.array([p[1] * dx for p in pts]) + 0.5 * dx - yc
+    mode, _ = slab_mode_source(x=ys, w=wg, n_WG=np.sqrt(12.25), n0=np.sqrt(2.085), wavelength=1.55 * µm, ind_m=0)
+    import torch
+
+    rho = np.stack([gaussian_filter(torch.rand((r, r), generator=torch.Generator().manual_seed(seed + b),
+                                               dtype=torch.float64).numpy(), sigma=3) for b in range(n_designs)])
+    return dict(eps_base=grid.permittivity, sigma=grid.conductivity, dx=dx, dt=t[1] - t[0], n_steps=n_steps,
+                sources=[src], monitor=mon, mode_profile=mode, frequency=f0, region=(y0, x0, r, r), rho0=rho,
+                eps_lo=2.085, eps_hi=12.25, design=d)

@@ -88,3 +88,31 @@ def test_autograd_function(bz):
     (J * torch.tensor([1.0, -2.0], dtype=torch.float64)).sum().backward()
     _, g = prob.value_and_grad(er)
     np.testing.assert_allclose(x.grad.numpy(), g * np.array([1.0, -2.0])[:, None, None], rtol=1e-12)
+
+
+def test_optimizer_improves_objective(bz):
+    from beamz_b200.optimization.topo2d import TopologyOptimizer2D
+
+    prob, er, *_ = _problem(bz, B=2, precision="fp32", n_steps=300, K=100, seed=5)
+    rho0 = (er - 2.085) / 10.165
+    opt = TopologyOptimizer2D(prob, rho0, 2.085, 12.25, lr=0.05, radius=1, steps=6)
+    J0 = opt.step()
+    for _ in range(4):
+        J = opt.step()
+    assert np.all(J > J0)
+
+
+def test_exact_gradient_vs_reference_heuristic(bz):
+    """The reference's estimate (examples/4_topo.py) is not the derivative of this
+    objective; record how it lines up with the exact gradient."""
+    from oracle.topo_heuristic import heuristic_gradient
+
+    prob, er, eps, sigma, dx, dt, n_steps, src, mon, mode, f0, region = _problem(bz, n_steps=360)
+    _, g = prob.value_and_grad(er)
+    y0, x0, h, w = region
+    e = eps.copy()
+    e[y0:y0 + h, x0:x0 + w] = er[0]
+    gh = heuristic_gradient(e, sigma, dx, dt, n_steps, [src], mon, mode, region)
+    cos = float(np.sum(g[0] * gh) / (np.linalg.norm(g[0]) * np.linalg.norm(gh)))
+    print(f"cosine(exact adjoint, reference heuristic) = {cos:.3f}")
+    assert np.isfinite(cos) and np.abs(gh).max() > 0
