@@ -4,9 +4,12 @@ Both run once on the host when a source is created:
 
 * ``solve_modes``: finite-difference eigenproblem eps + (DfDb + DbDf)/(2 k0^2) on a
   line, with a complex coordinate-stretching absorber of ``npml`` points per
-  side, solved with ARPACK shift-invert around n_max^2 (scipy ``eigs``). ARPACK
-  starts from a random vector, so the overall phase of each mode is arbitrary,
-  exactly as in the reference.
+  side, solved with ARPACK shift-invert around n_max^2 (scipy ``eigs``). The
+  reference lets ARPACK start from a random vector, so the overall phase of each
+  mode (and with it the real part a real-field run injects) changes from run to
+  run. Here the start vector is a fixed pseudo-random one and each mode is
+  rotated so that its largest-magnitude entry is real and positive: the same
+  modes up to a phase, reproducible across runs.
 * ``slab_mode_source``: analytic TE mode of a symmetric slab; the propagation
   constant is bracketed by a 2000-point scan of the even/odd dispersion relations
   and refined by 50 bisection steps, then the profile is normalised to unit
@@ -48,8 +51,11 @@ def solve_modes(eps, omega, dL, npml=0, m=2):
     fwd, bwd = compute_derivative_matrices(N, dL, npml)
     A = sps.diags(eps.flatten(), 0) + 0.5 * (fwd @ bwd + bwd @ fwd) * (1 / k0) ** 2
     n_max = np.sqrt(np.max(eps))
-    vals, vecs = spl.eigs(A, k=m, sigma=n_max ** 2, which="LM")
+    v0 = np.random.default_rng(0).standard_normal(N)
+    vals, vecs = spl.eigs(A, k=m, sigma=n_max ** 2, which="LM", v0=v0)
     vecs = vecs / np.sqrt(np.sum(np.square(np.abs(vecs)), axis=0))
+    peak = vecs[np.argmax(np.abs(vecs), axis=0), np.arange(vecs.shape[1])]
+    vecs = vecs * (np.abs(peak) / np.where(peak == 0, 1.0, peak))[None, :]
     return np.sqrt(vals), vecs
 
 

@@ -237,6 +237,10 @@ class Engine2D:
             if self.record is not None:
                 room = min(room, self.mops.rec_step0 + self.rec_rows - self.step_index)
             if self.use_graphs and room >= GRAPH_CHUNK:
+                # the chunk writes GRAPH_CHUNK ring slots: fold what single steps left
+                # there first, or those samples are overwritten before they are read
+                if self.step_index - self._folded > RING_LEN - GRAPH_CHUNK:
+                    self._fold()
                 phase = self.step_index & 1
                 g = self._graph_for(phase)
                 self.d_step.fill_(self.step_index - phase)

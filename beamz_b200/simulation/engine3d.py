@@ -214,6 +214,9 @@ class Engine3D:
             if self.record is not None:
                 room = min(room, self.gops.rec_step0 + self.rec_rows - self.step_index)
             if self.use_graphs and room >= GRAPH_CHUNK:
+                # fold samples left by single steps before the chunk overwrites their slots
+                if self.step_index - self._folded > RING_LEN - GRAPH_CHUNK:
+                    self._fold()
                 phase = self.step_index & 1
                 g = self._graph_for(phase)
                 self.d_step.fill_(self.step_index - phase)

@@ -38,8 +38,10 @@ def _problem(bz, B=1, precision="fp64", n_steps=360, K=128, seed=0):
     return prob, er, eps, sigma, dx, dt, n_steps, src, mon, mode, f0, region
 
 
-def test_adjoint_matches_central_differences_fp64(bz):
-    prob, er, *_ = _problem(bz)
+# K = 100 leaves single steps between graph chunks at every checkpoint
+@pytest.mark.parametrize("K", [128, 100])
+def test_adjoint_matches_central_differences_fp64(bz, K):
+    prob, er, *_ = _problem(bz, K=K)
     J, g = prob.value_and_grad(er)
     rng = np.random.default_rng(99)
     h = 1e-3
@@ -53,8 +55,9 @@ def test_adjoint_matches_central_differences_fp64(bz):
     assert np.abs(g).max() > 0 and J[0] > 0
 
 
-def test_objective_matches_oracle(bz):
-    prob, er, eps, sigma, dx, dt, n_steps, src, mon, mode, f0, region = _problem(bz)
+@pytest.mark.parametrize("K", [128, 100])
+def test_objective_matches_oracle(bz, K):
+    prob, er, eps, sigma, dx, dt, n_steps, src, mon, mode, f0, region = _problem(bz, K=K)
     J = prob.forward(er)
     y0, x0, h, w = region
     e = eps.copy()
@@ -115,4 +118,5 @@ def test_exact_gradient_vs_reference_heuristic(bz):
     gh = heuristic_gradient(e, sigma, dx, dt, n_steps, [src], mon, mode, region)
     cos = float(np.sum(g[0] * gh) / (np.linalg.norm(g[0]) * np.linalg.norm(gh)))
     print(f"cosine(exact adjoint, reference heuristic) = {cos:.3f}")
-    assert np.isfinite(cos) and np.abs(gh).max() > 0
+    # measured -0.93 here: the estimate tracks the exact gradient up to its sign
+    assert np.isfinite(cos) and abs(cos) > 0.5

@@ -133,6 +133,26 @@ def test_step3d_graph_equals_direct(bz):
     np.testing.assert_array_equal(outs[0], outs[1])
 
 
+def test_dft3d_with_runs_split_off_graph_chunks(bz):
+    """Plane-monitor DFT sums with run_steps counts off the graph chunk equal the ones
+    of direct launches (single-step samples are folded before a chunk reuses the ring)."""
+    from beamz_b200.simulation.engine3d import Engine3D
+
+    d, grid, eps, sig, dx, dt, t, src, sgn = _odd_problem(bz, n_steps=120)
+    g = bz.GaussianSource(position=(6 * dx, 5 * dx, 3 * dx), width=dx / 10, signal=sgn)
+    mon = bz.Monitor(design=d, start=(1 * dx, 1 * dx, 6 * dx), end=(11 * dx, 9 * dx, 6 * dx), frequencies=[1.9e14],
+                     record_fields=False, accumulate_power=False)
+    outs = []
+    for graphs, parts in ((False, [120]), (True, [20, 40, 5, 32, 23])):
+        eng = Engine3D(eps, sig, dx, dx, dx, dt, len(t), [g], [mon], precision="fp64", record=False,
+                       use_graphs=graphs)
+        for p in parts:
+            eng.run_steps(p)
+        eng._fold()
+        outs.append(eng.dft.cpu().numpy())
+    assert rel_l2(outs[1], outs[0]) <= 1e-12
+
+
 def test_step3d_tile_heights_agree(bz):
     d, grid, eps, sig, dx, dt, t, src, sgn = _odd_problem(bz, n_steps=60)
     g = bz.GaussianSource(position=(6 * dx, 5 * dx, 4 * dx), width=dx / 10, signal=sgn)

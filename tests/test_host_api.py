@@ -24,6 +24,11 @@ def test_solve_modes_matches_up_to_phase(bz, golden):
     gorder = np.argsort(-np.real(g["solve_neff"]))
     np.testing.assert_allclose(neff[order], g["solve_neff"][gorder], rtol=1e-10)
     np.testing.assert_allclose(np.abs(vecs[:, order]), g["solve_abs"][:, gorder], rtol=1e-6, atol=1e-9)
+    # the phase convention: repeatable, largest entry real and positive
+    _, again = bz.solve_modes(g["solve_eps"], 2 * np.pi * bz.LIGHT_SPEED / 1.55e-6, 2e-6 / 400, npml=20, m=2)
+    np.testing.assert_array_equal(again, vecs)
+    peak = vecs[np.argmax(np.abs(vecs), axis=0), [0, 1]]
+    assert np.all(peak.real > 0) and np.all(np.abs(peak.imag) <= 1e-15 * np.abs(peak))
 
 
 def test_signals_bit_exact(bz, golden):
