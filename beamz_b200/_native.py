@@ -106,6 +106,8 @@ _version = _sig("bz_version", C.c_char_p, [])
 _last_error = _sig("bz_last_error", C.c_int, [C.c_char_p, C.c_size_t])
 _step2d = _sig("bz_step2d", C.c_int, [C.POINTER(Grid2D), C.POINTER(Fields2D), C.POINTER(SourceOps),
                                        C.POINTER(MonitorOps), i64, vp, vp])
+_step2d_multi = _sig("bz_step2d_multi", C.c_int, [C.POINTER(Grid2D), C.POINTER(Fields2D), C.POINTER(SourceOps),
+                                                   C.POINTER(MonitorOps), i64, i32, i32, vp, vp])
 _dft_fold = _sig("bz_dft_fold", C.c_int, [vp, i32, i32, i64, i32, vp, i64, i64, i32, vp, vp])
 _step2d_dft_static = _sig("bz_step2d_dft_static", C.c_int,
                           [C.POINTER(Grid2D), C.POINTER(Fields2D), C.POINTER(SourceOps), C.POINTER(MonitorOps), i64,
@@ -127,7 +129,7 @@ _raster2d = _sig("bz_rasterize2d", C.c_int, [i32, i32, vp, vp, vp, vp, vp, vp, i
                                               f64, f64, f64, vp, vp, vp, vp])
 
 #: every symbol include/beamz_b200.h declares (checked by the CPU test suite)
-EXPORTED = ["bz_version", "bz_last_error", "bz_step2d", "bz_dft_fold", "bz_step2d_dft_static", "bz_advance_step",
+EXPORTED = ["bz_version", "bz_last_error", "bz_step2d", "bz_step2d_multi", "bz_dft_fold", "bz_step2d_dft_static", "bz_advance_step",
             "bz_adjoint_step2d", "bz_step3d", "bz_cell_ops", "bz_gather", "bz_power3d", "bz_dft_fold_q", "bz_rasterize3d", "bz_prepare_coeffs", "bz_update_h2d",
             "bz_update_e2d", "bz_rasterize2d"]
 
@@ -157,6 +159,11 @@ def version() -> str:
 def step2d(grid, fields, src, mon, step: int, d_step: int | None, stream: int) -> None:
     check(_step2d(C.byref(grid), C.byref(fields), C.byref(src) if src is not None else None,
                   C.byref(mon) if mon is not None else None, step, d_step, stream))
+
+
+def step2d_multi(grid, fields, src, mon, step: int, n_sub: int, tile: int, d_step: int | None, stream: int) -> None:
+    check(_step2d_multi(C.byref(grid), C.byref(fields), C.byref(src) if src is not None else None,
+                        C.byref(mon) if mon is not None else None, step, n_sub, tile, d_step, stream))
 
 
 def advance_step(d_step: int, n: int, stream: int) -> None:

@@ -21,6 +21,31 @@ __device__ __forceinline__ void h_coeffs(T a, T chx, T chy, T& fh, T& cx, T& cy)
   }
 }
 
+// Explicitly rounded arithmetic, so that every kernel evaluating an update gets
+// the same bits whatever the compiler would contract in its context.
+__device__ __forceinline__ float fma_rn(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+__device__ __forceinline__ double fma_rn(double a, double b, double c) { return __fma_rn(a, b, c); }
+__device__ __forceinline__ float mul_rn(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ double mul_rn(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ float sub_rn(float a, float b) { return __fsub_rn(a, b); }
+__device__ __forceinline__ double sub_rn(double a, double b) { return __dsub_rn(a, b); }
+
+// Hx' = fh*Hx - cx*(Ez(x+1) - Ez(x))   (numpy_backend.py:55-57)
+template <typename T>
+__device__ __forceinline__ T hx_update(T fh, T hx, T cx, T ez_right, T ez) {
+  return fma_rn(fh, hx, -mul_rn(cx, sub_rn(ez_right, ez)));
+}
+// Hy' = fh*Hy + cy*(Ez(y+1) - Ez(y))   (numpy_backend.py:58-60)
+template <typename T>
+__device__ __forceinline__ T hy_update(T fh, T hy, T cy, T ez_down, T ez) {
+  return fma_rn(fh, hy, mul_rn(cy, sub_rn(ez_down, ez)));
+}
+// Ez' = fe*Ez + ce*(-(Hx - Hx(x-1)) + qy*(Hy - Hy(y-1)))   (numpy_backend.py:80-88)
+template <typename T>
+__device__ __forceinline__ T ez_update(T fe, T ez, T ce, T qy, T hx, T hx_left, T hy, T hy_up) {
+  return fma_rn(fe, ez, mul_rn(ce, fma_rn(qy, sub_rn(hy, hy_up), -sub_rn(hx, hx_left))));
+}
+
 __device__ __forceinline__ int lower_bound_i(const int* a, int lo, int hi, int key) {
   while (lo < hi) {
     const int mid = (lo + hi) >> 1;

@@ -2,8 +2,10 @@
 
 Holds the ping-pong field buffers ([design][component][ny][pitch], x contiguous,
 pitch a multiple of 32 elements), the update coefficients, the compiled source
-and monitor operations, and drives ``bz_step2d``: one launch per time step,
-replayed in CUDA-graph chunks when no host work is due between steps.
+and monitor operations, and drives the step kernels: ``bz_step2d_multi`` advances
+``time_block`` steps per launch (temporal blocking), ``bz_step2d`` one step (single
+steps, power accumulation, region capture); launches are replayed in CUDA-graph
+chunks when no host work is due between steps.
 """
 from __future__ import annotations
 
@@ -16,7 +18,7 @@ from .. import _native as nat
 from ..const import EPS_0, MU_0
 from .compile_ops import SourceOps, compile_monitors_2d, compile_sources
 
-GRAPH_CHUNK = 64  # steps per captured graph (even: keeps ping-pong parity)
+GRAPH_CHUNK = 64  # at most this many steps per captured graph
 RING_LEN = GRAPH_CHUNK  # monitor samples kept between DFT folds
 
 
@@ -26,7 +28,8 @@ def _round_up(n: int, m: int) -> int:
 
 class Engine2D:
     def __init__(self, eps_r, sigma, dx, dy, dt, n_steps, sources, monitors, *, precision="fp32", n_comp=None,
-                 power=False, n_designs=1, record=True, use_graphs=True, device=None, tile_rows=16):
+                 power=False, n_designs=1, record=True, use_graphs=True, device=None, tile_rows=16, time_block=7,
+                 tb_tile=0):
         if not torch.cuda.is_available():
             raise RuntimeError("beamz_b200 needs a CUDA GPU (sm_100a); none is visible")
         self.dev = torch.device("cuda", torch.cuda.current_device()) if device is None else torch.device(device)
@@ -65,6 +68,12 @@ class Engine2D:
         self.d_step = torch.zeros(1, dtype=torch.int64, device=self.dev)
         self.use_graphs = use_graphs
         self._graphs: dict[int, torch.cuda.CUDAGraph] = {}
+        if int(time_block) not in (1, 3, 5, 7):
+            raise ValueError(f"time_block must be 1, 3, 5 or 7 (got {time_block})")
+        # power accumulation runs on the single-step kernel
+        self.time_block = 1 if power else int(time_block)
+        self.tb_tile = int(tb_tile)
+        self.chunk = GRAPH_CHUNK // self.time_block * self.time_block  # steps per graph
         g = nat.Grid2D()
         g.nx, g.ny, g.pitch = self.nx, self.ny, self.pitch
         g.n_designs, g.n_comp, g.n_mat, g.dtype = n_designs, n_comp, self.n_mat, self.bz_dtype
@@ -181,6 +190,15 @@ class Engine2D:
         nat.step2d(self.grid, self._fields(), self.sops if self.sops.n_ops else None,
                    self.mops if self.mops.n_points else None, step_arg, d_step_ptr, self._stream())
 
+    def _launch_tb(self, step_arg: int, d_step_ptr):
+        nat.step2d_multi(self.grid, self._fields(), self.sops if self.sops.n_ops else None,
+                         self.mops if self.mops.n_points else None, step_arg, self.time_block, self.tb_tile,
+                         d_step_ptr, self._stream())
+
+    def _block(self) -> int:
+        """Steps per launch available now (the capture box needs single steps)."""
+        return 1 if self.mops.region else self.time_block
+
     def step_once(self):
         """Advance one time step with a direct launch."""
         self._maybe_drain()
@@ -215,16 +233,17 @@ class Engine2D:
             self._graphs.clear()
 
     def _graph_for(self, phase: int) -> torch.cuda.CUDAGraph:
-        """Graph of GRAPH_CHUNK launches starting at a step of parity `phase`; the
-        time index comes from the device counter (d_step = first step - phase)."""
+        """Graph of the launches of `chunk` steps starting at a step of parity `phase`;
+        the time index comes from the device counter (d_step = first step - phase)."""
         g = self._graphs.get(phase)
         if g is None:
             g = torch.cuda.CUDAGraph()
             s = torch.cuda.Stream()
             s.wait_stream(torch.cuda.current_stream())
+            tb = self.time_block
             with torch.cuda.stream(s), torch.cuda.graph(g, stream=s):
-                for k in range(GRAPH_CHUNK):
-                    self._launch(phase + k, self.d_step.data_ptr())
+                for k in range(0, self.chunk, tb):
+                    (self._launch_tb if tb > 1 else self._launch)(phase + k, self.d_step.data_ptr())
             torch.cuda.current_stream().wait_stream(s)
             self._graphs[phase] = g
         return g
@@ -236,18 +255,26 @@ class Engine2D:
             room = n
             if self.record is not None:
                 room = min(room, self.mops.rec_step0 + self.rec_rows - self.step_index)
-            if self.use_graphs and room >= GRAPH_CHUNK:
-                # the chunk writes GRAPH_CHUNK ring slots: fold what single steps left
+            tb = self._block()
+            if self.use_graphs and tb == self.time_block and room >= self.chunk:
+                # the chunk writes `chunk` ring slots: fold what earlier launches left
                 # there first, or those samples are overwritten before they are read
-                if self.step_index - self._folded > RING_LEN - GRAPH_CHUNK:
+                if self.step_index - self._folded > RING_LEN - self.chunk:
                     self._fold()
                 phase = self.step_index & 1
                 g = self._graph_for(phase)
                 self.d_step.fill_(self.step_index - phase)
                 g.replay()
-                self.step_index += GRAPH_CHUNK
-                n -= GRAPH_CHUNK
+                self.step_index += self.chunk
+                n -= self.chunk
                 self._fold()
+                continue
+            if tb > 1 and room >= tb:
+                if self.step_index - self._folded > RING_LEN - tb:
+                    self._fold()
+                self._launch_tb(self.step_index, None)
+                self.step_index += tb
+                n -= tb
                 continue
             self.step_once()
             n -= 1

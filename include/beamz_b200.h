@@ -147,6 +147,20 @@ typedef struct bz_monitor_ops {
 int bz_step2d(const bz_grid2d* g, const bz_fields2d* f, const bz_source_ops* src,
               const bz_monitor_ops* mon, int64_t step, const int64_t* d_step, void* stream);
 
+/* n_sub consecutive steps of bz_step2d in one launch (temporal blocking; replaces
+ * n_sub iterations of the reference's step loop, fdtd.py:188-198 + helper.py). Same
+ * results as n_sub bz_step2d calls from `step` (same arithmetic per cell; sources,
+ * monitor records and ring samples per sub-step). Each block keeps a tile of the
+ * grid in registers for all sub-steps and stores the part of it that stays exact.
+ * n_sub: 1, 3, 5 or 7 (odd, so the copy read stays (step & 1) and the result lands
+ * in copy ((step + n_sub) & 1)); 1 is bz_step2d. tile: 0 = default, 1..3 = tile
+ * shapes of 4x8, 4x16 and 8x8 (rows per warp x warps) for float32 single-component
+ * fields. Power accumulation and region capture return BZ_ERR_UNSUPPORTED (use
+ * bz_step2d for those steps). */
+int bz_step2d_multi(const bz_grid2d* g, const bz_fields2d* f, const bz_source_ops* src,
+                    const bz_monitor_ops* mon, int64_t step, int32_t n_sub, int32_t tile,
+                    const int64_t* d_step, void* stream);
+
 /* Folds `count` consecutive ring samples, steps step0 .. step0+count-1 (ring slot
  * step % ring_len, count <= ring_len), into float64 DFT sums:
  *   dft[i][f][q] += sum_s ring[s % ring_len][i][q] * phasor[s][f][E or H]

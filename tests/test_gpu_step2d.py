@@ -115,6 +115,69 @@ def test_step2d_odd_grid_complex_vs_oracle(bz, precision, tol):
     assert np.abs(got_ez - rec["Ez"]).max() <= tol * np.abs(rec["Ez"]).max()
 
 
+def _tiled_problem(bz, seed=21, n_steps=160):
+    """83x141 grid (several temporal tiles each way) with a complex line source, a
+    Gaussian source straddling tile edges, and two monitors on tile edges."""
+    from beamz_b200.devices.sources import ModeSource
+
+    eps, sigma, dx, dt, t, sig, Pt = _random_problem(seed, ny=83, nx=141, n_steps=n_steps)
+    src = ModeSource.__new__(ModeSource)
+    src.__dict__.update(direction="+x", enforce_direction=True, signal=sig, mode_profiles=Pt.mode_profiles)
+    g = bz.GaussianSource(position=(54 * dx, 54 * dx), width=dx / 10, signal=sig)
+    freqs = np.array([1.8e14, 2.0e14])
+    mv = bz.Monitor(start=(54 * dx, 2 * dx), end=(54 * dx, 80 * dx), frequencies=freqs)
+    mh = bz.Monitor(start=(3 * dx, 50 * dx), end=(137 * dx, 50 * dx), frequencies=freqs)
+    return eps, sigma, dx, dt, t, [src, g], [mv, mh], freqs
+
+
+@pytest.mark.parametrize("tb,tile", [(1, 0), (3, 1), (5, 2), (5, 3), (7, 0)])
+@pytest.mark.parametrize("precision,tol", [("fp64", 1e-11), ("fp32", 2e-5)])
+def test_time_blocked_run_vs_oracle(bz, tb, tile, precision, tol):
+    eps, sigma, dx, dt, t, srcs, mons, freqs = _tiled_problem(bz)
+    sim = _sim_from_arrays(bz, eps, sigma, dx, t, srcs, mons, precision, time_block=tb, tb_tile=tile)
+    sim.run(live=False, save=False, save_memory_mode=True)
+    assert sim.engine.time_block == tb
+    ref = fdtd2d.run(eps, sigma, dx, dx, dt, len(t), srcs, mons, dft_freqs=freqs)
+    assert rel_l2(sim.engine.field("Ez").cpu().numpy(), ref["Ez"]) <= tol
+    assert rel_l2(sim.engine.field("Hx").cpu().numpy(), ref["Hx"]) <= tol
+    assert rel_l2(sim.engine.field("Hy").cpu().numpy(), ref["Hy"]) <= tol
+    for m, rec in zip(mons, ref["records"]):
+        for k in ("Ez", "Hx", "Hy"):
+            got = np.array([np.asarray(v) for v in m.fields[k]])
+            assert np.abs(got - rec[k]).max() <= tol * np.abs(rec[k]).max(), k
+    # DFT sums of the real field (component 0): [points][freq][5] per monitor block
+    d = sim.engine.dft_fields()[0, 0]
+    for i, (sl, dft) in enumerate(zip(sim.engine.mp.slices, ref["dft"])):
+        got = d[sl, i * len(freqs):(i + 1) * len(freqs)].transpose(1, 0, 2)
+        errs = [rel_l2(got[..., q], dft[..., q]) for q in range(5)]
+        assert max(errs) <= 10 * tol, (i, errs)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_time_blocked_batch_matches_single_steps(bz, precision):
+    """Batched designs with their own materials: time-blocked launches (graphs and
+    direct, split runs) give the same bits as single-step launches for fields and
+    records (both kernels round every operation explicitly); DFT sums differ only by
+    the grouping of the float64 fold."""
+    from beamz_b200.simulation.engine2d import Engine2D
+
+    eps, sigma, dx, dt, t, srcs, mons, freqs = _tiled_problem(bz, seed=23, n_steps=150)
+    rng = np.random.default_rng(5)
+    eps_b = np.stack([eps, eps[::-1, :], 1.0 + 11.0 * rng.random(eps.shape)])
+    outs = []
+    for tb, graphs, parts in ((1, False, [150]), (5, True, [71, 64, 15]), (7, False, [150]), (3, True, [150])):
+        eng = Engine2D(eps_b, sigma, dx, dx, dt, len(t), srcs, mons, precision=precision, n_comp=2, n_designs=3,
+                       record=True, use_graphs=graphs, time_block=tb)
+        for p in parts:
+            eng.run_steps(p)
+        outs.append(([eng.field(k, d).cpu().numpy() for k in ("Ez", "Hx", "Hy") for d in range(3)]
+                     + [eng.take_records()], eng.dft_fields()))
+    for exact, dft in outs[1:]:
+        for a, b in zip(exact, outs[0][0]):
+            np.testing.assert_array_equal(a, b)
+        assert rel_l2(dft, outs[0][1]) <= 1e-12
+
+
 def test_graph_replay_equals_direct_launches(bz):
     eps, sigma, dx, dt, t, sig, _ = _random_problem(5, n_steps=300)
     src = bz.GaussianSource(position=(18 * dx, 14 * dx), width=dx / 10, signal=sig)

@@ -38,7 +38,7 @@ def _engine(bz):
                        accumulate_power=False),
             bz.Monitor(start=(5 * dx, 30 * dx), end=(45 * dx, 30 * dx), frequencies=freqs, record_fields=False,
                        accumulate_power=False)]
-    sim = bz.FDTD(design=grid, time=t, devices=mons, backend_options={"graph": False})
+    sim = bz.FDTD(design=grid, time=t, devices=mons, backend_options={"graph": False, "time_block": 1})
     sim.sources = [bz.GaussianSource(position=(15 * dx, 20 * dx), width=dx / 10, signal=sig)]
     sim.initialize_simulation(save=False, live=False, save_memory_mode=True)
     return sim.engine
