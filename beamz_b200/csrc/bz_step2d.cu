@@ -293,8 +293,11 @@ __global__ void __launch_bounds__(32 * NW) step2d_tb_kernel(
   xs[0] = X0 + lane;
   xs[1] = X0 + 32 + lane;
   T ez[R][2][NC], hx[R][2][NC], hy[R][2][NC];
+  // Cells whose H or E the reference never changes (Hx in the last column, Hy in the
+  // last row, E on the PEC ring, everything outside the grid) get factors that keep
+  // the value: cx = 0 / cy = 0 for H (those values start and stay zero), fe = 1 and
+  // ce = 0 for E. The sub-step loop then needs no per-cell masks.
   T fh[R][2], cx[R][2], cy[R][2], fe[R][2], cc[R][2];
-  unsigned hx_ok = 0u, hy_ok = 0u, e_in = 0u;
 #pragma unroll
   for (int i = 0; i < R; ++i) {
     const int y = yb + i;
@@ -306,19 +309,18 @@ __global__ void __launch_bounds__(32 * NW) step2d_tb_kernel(
       const T a = in ? __ldg(loss + mb + r) : T(0);
       const T c = in ? __ldg(ce + mb + r) : T(0);
       h_coeffs(a, g.chx, g.chy, fh[i][j], cx[i][j], cy[i][j]);
-      fe[i][j] = sub_rn(T(1), mul_rn(mul_rn(a, c), g.inv_kd2));
-      cc[i][j] = c;
+      const bool interior = x >= 1 && x <= nx - 2 && y >= 1 && y <= ny - 2;
+      fe[i][j] = interior ? sub_rn(T(1), mul_rn(mul_rn(a, c), g.inv_kd2)) : T(1);
+      cc[i][j] = interior ? c : T(0);
+      if (!(in && x < nx - 1)) cx[i][j] = T(0);
+      if (!(in && y < ny - 1)) cy[i][j] = T(0);
 #pragma unroll
       for (int k = 0; k < NC; ++k) {
         const long long off = fb + k * g.plane + r;
         ez[i][j][k] = in ? __ldg(ez_in + off) : T(0);
-        hx[i][j][k] = in ? __ldg(hx_in + off) : T(0);
-        hy[i][j][k] = in ? __ldg(hy_in + off) : T(0);
+        hx[i][j][k] = (in && x < nx - 1) ? __ldg(hx_in + off) : T(0);
+        hy[i][j][k] = (in && y < ny - 1) ? __ldg(hy_in + off) : T(0);
       }
-      const unsigned bit = 1u << (i * 2 + j);
-      if (in && x < nx - 1) hx_ok |= bit;
-      if (in && y < ny - 1) hy_ok |= bit;
-      if (x >= 1 && x <= nx - 2 && y >= 1 && y <= ny - 2) e_in |= bit;
     }
   }
   // Operation ranges: sources over the tile's columns, monitors over the owned ones.
@@ -386,11 +388,8 @@ __global__ void __launch_bounds__(32 * NW) step2d_tb_kernel(
         }
 #pragma unroll
         for (int j = 0; j < 2; ++j) {
-          const unsigned bit = 1u << (i * 2 + j);
-          const T hxn = hx_update(fh[i][j], hx[i][j][k], cx[i][j], er[j], ez[i][j][k]);
-          const T hyn = hy_update(fh[i][j], hy[i][j][k], cy[i][j], ed[j], ez[i][j][k]);
-          hx[i][j][k] = (hx_ok & bit) ? hxn : T(0);
-          hy[i][j][k] = (hy_ok & bit) ? hyn : T(0);
+          hx[i][j][k] = hx_update(fh[i][j], hx[i][j][k], cx[i][j], er[j], ez[i][j][k]);
+          hy[i][j][k] = hy_update(fh[i][j], hy[i][j][k], cy[i][j], ed[j], ez[i][j][k]);
         }
       }
     }
@@ -419,10 +418,8 @@ __global__ void __launch_bounds__(32 * NW) step2d_tb_kernel(
           hu[0] = hu[1] = T(0);
         }
 #pragma unroll
-        for (int j = 0; j < 2; ++j) {
-          if (e_in & (1u << (i * 2 + j)))
-            ez[i][j][k] = ez_update(fe[i][j], ez[i][j][k], cc[i][j], g.qy, hx[i][j][k], hl[j], hy[i][j][k], hu[j]);
-        }
+        for (int j = 0; j < 2; ++j)
+          ez[i][j][k] = ez_update(fe[i][j], ez[i][j][k], cc[i][j], g.qy, hx[i][j][k], hl[j], hy[i][j][k], hu[j]);
       }
     }
     // Sources (helper.py:5-118), in operation order per cell

@@ -74,6 +74,8 @@ class Engine2D:
         self.time_block = 1 if power else int(time_block)
         self.tb_tile = int(tb_tile)
         self.chunk = GRAPH_CHUNK // self.time_block * self.time_block  # steps per graph
+        self.n_step_launches = 0  # step-kernel launches issued (graph nodes included)
+        self.n_fold_launches = 0
         g = nat.Grid2D()
         g.nx, g.ny, g.pitch = self.nx, self.ny, self.pitch
         g.n_designs, g.n_comp, g.n_mat, g.dtype = n_designs, n_comp, self.n_mat, self.bz_dtype
@@ -203,6 +205,7 @@ class Engine2D:
         """Advance one time step with a direct launch."""
         self._maybe_drain()
         self._launch(self.step_index, None)
+        self.n_step_launches += 1
         self.step_index += 1
         if self.dft is not None and self.step_index - self._folded >= RING_LEN:
             self._fold()
@@ -214,6 +217,7 @@ class Engine2D:
             nat.dft_fold(self.ring.data_ptr(), self.bz_dtype, RING_LEN, self.n_designs * self.n_comp * self.mp.n_points,
                          len(self.freqs), self.phasor.data_ptr(), self.n_steps, self._folded, cnt,
                          self.dft.data_ptr(), self._stream())
+            self.n_fold_launches += 1
             self._folded += cnt
 
     def reset(self):
@@ -265,6 +269,7 @@ class Engine2D:
                 g = self._graph_for(phase)
                 self.d_step.fill_(self.step_index - phase)
                 g.replay()
+                self.n_step_launches += self.chunk // self.time_block
                 self.step_index += self.chunk
                 n -= self.chunk
                 self._fold()
@@ -273,6 +278,7 @@ class Engine2D:
                 if self.step_index - self._folded > RING_LEN - tb:
                     self._fold()
                 self._launch_tb(self.step_index, None)
+                self.n_step_launches += 1
                 self.step_index += tb
                 n -= tb
                 continue
