@@ -40,16 +40,22 @@ def build(verbose: bool = False, force: bool = False) -> Path:
     nvcc = _nvcc()
     OBJ.mkdir(exist_ok=True)
     hdr_mtime = max((p.stat().st_mtime for p in _headers()), default=0.0)
-    objs = []
+    objs, cmds = [], []
     for src in sorted(CSRC.glob("*.cu")):
         obj = OBJ / (src.stem + ".o")
         objs.append(obj)
         if not force and obj.exists() and obj.stat().st_mtime >= max(src.stat().st_mtime, hdr_mtime):
             continue
-        cmd = [nvcc, *ARCH, *CFLAGS, "-I", str(ROOT / "include"), "-c", str(src), "-o", str(obj)]
+        cmds.append([nvcc, *ARCH, *CFLAGS, "-I", str(ROOT / "include"), "-c", str(src), "-o", str(obj)])
+    # compile the translation units concurrently (each nvcc is single-threaded)
+    procs = []
+    for cmd in cmds:
         if verbose:
             print(" ".join(cmd), flush=True)
-        subprocess.run(cmd, check=True)
+        procs.append((cmd, subprocess.Popen(cmd)))
+    failed = [cmd for cmd, p in procs if p.wait() != 0]
+    if failed:
+        raise subprocess.CalledProcessError(1, failed[0])
     if force or not LIB.exists() or LIB.stat().st_mtime < max(o.stat().st_mtime for o in objs):
         cmd = [nvcc, *ARCH, "-shared", "-o", str(LIB), *map(str, objs), "-lcudart"]
         if verbose:

@@ -63,6 +63,14 @@ class Adjoint2D(C.Structure):
                 ("fwd_step0", i64), ("n_fwd", i32), ("reserved", i32)]
 
 
+class Gemm(C.Structure):
+    _fields_ = [("M", i32), ("N", i32), ("K", i32), ("batch", i32), ("splitk", i32), ("act", i32), ("ta", i32),
+                ("tb", i32), ("atomic", i32), ("reserved", i32), ("A", vp), ("lda", i64), ("sa", i64), ("B", vp),
+                ("ldb", i64), ("sb", i64), ("alpha", C.c_float), ("reserved2", C.c_float), ("cadd", vp),
+                ("ldadd", i64), ("sadd", i64), ("bias_m", vp), ("bias_n", vp), ("outf", vp), ("outh", vp),
+                ("ldc", i64), ("sc", i64), ("pre", vp), ("ldpre", i64), ("spre", i64)]
+
+
 class Grid3D(C.Structure):
     _fields_ = [("nx", i32), ("ny", i32), ("nz", i32), ("pitch", i32), ("n_designs", i32), ("n_comp", i32),
                 ("n_mat", i32), ("dtype", i32), ("tile_z", i32), ("reserved", i32), ("chx", f64), ("chy", f64),
@@ -127,11 +135,22 @@ _upd_h2d = _sig("bz_update_h2d", C.c_int, [i32, i32, i32, i32, vp, vp, vp, vp, f
 _upd_e2d = _sig("bz_update_e2d", C.c_int, [i32, i32, i32, i32, vp, vp, vp, vp, vp, f64, f64, f64, f64, vp])
 _raster2d = _sig("bz_rasterize2d", C.c_int, [i32, i32, vp, vp, vp, vp, vp, vp, i32, vp, vp, vp, vp, i32, vp,
                                               f64, f64, f64, vp, vp, vp, vp])
+_gemm = _sig("bz_gemm_bf16", C.c_int, [C.POINTER(Gemm), vp])
+_spec = _sig("bz_spectral_mix", C.c_int, [vp, vp, vp, i32, i32, i32, i32, vp])
+_spec_bwd = _sig("bz_spectral_mix_bwd", C.c_int, [vp, vp, vp, vp, vp, i32, i32, i32, i32, vp])
+_gelu_bwd = _sig("bz_gelu_bwd", C.c_int, [vp, vp, vp, i64, vp])
+_row_mean = _sig("bz_row_mean", C.c_int, [vp, vp, i64, i32, C.c_float, vp])
+_row_bcast = _sig("bz_row_broadcast", C.c_int, [vp, vp, i64, i32, C.c_float, vp])
+_chan_sum = _sig("bz_chan_sum", C.c_int, [vp, vp, i32, i32, i32, vp])
+_adam = _sig("bz_adam", C.c_int, [vp, vp, vp, vp, vp, i64, C.c_float, C.c_float, C.c_float, C.c_float, i32,
+                                  C.c_float, vp])
+_to_bf16 = _sig("bz_to_bf16", C.c_int, [vp, vp, i64, vp])
 
 #: every symbol include/beamz_b200.h declares (checked by the CPU test suite)
 EXPORTED = ["bz_version", "bz_last_error", "bz_step2d", "bz_step2d_multi", "bz_dft_fold", "bz_step2d_dft_static", "bz_advance_step",
             "bz_adjoint_step2d", "bz_step3d", "bz_cell_ops", "bz_gather", "bz_power3d", "bz_dft_fold_q", "bz_rasterize3d", "bz_prepare_coeffs", "bz_update_h2d",
-            "bz_update_e2d", "bz_rasterize2d"]
+            "bz_update_e2d", "bz_rasterize2d", "bz_gemm_bf16", "bz_spectral_mix", "bz_spectral_mix_bwd", "bz_gelu_bwd",
+            "bz_row_mean", "bz_row_broadcast", "bz_chan_sum", "bz_adam", "bz_to_bf16"]
 
 
 class NativeError(RuntimeError):
@@ -216,3 +235,40 @@ def rasterize3d(*args) -> None:
 
 def adjoint_step2d(grid, state, ops, step, phase, stream) -> None:
     check(_adjoint2d(C.byref(grid), C.byref(state), C.byref(ops) if ops is not None else None, step, phase, stream))
+
+
+# ---- surrogate kernels -------------------------------------------------------------
+def gemm(g: Gemm, stream: int) -> None:
+    check(_gemm(C.byref(g), stream))
+
+
+def spectral_mix(U, W, O, B, ci, co, n_modes, stream) -> None:
+    check(_spec(U, W, O, B, ci, co, n_modes, stream))
+
+
+def spectral_mix_bwd(dO, U, W, dU, dW, B, ci, co, n_modes, stream) -> None:
+    check(_spec_bwd(dO, U, W, dU, dW, B, ci, co, n_modes, stream))
+
+
+def gelu_bwd(dy, pre, dx, n, stream) -> None:
+    check(_gelu_bwd(dy, pre, dx, n, stream))
+
+
+def row_mean(x, out, rows, P, scale, stream) -> None:
+    check(_row_mean(x, out, rows, P, scale, stream))
+
+
+def row_broadcast(g, x, rows, P, scale, stream) -> None:
+    check(_row_bcast(g, x, rows, P, scale, stream))
+
+
+def chan_sum(x, out, B, C_, P, stream) -> None:
+    check(_chan_sum(x, out, B, C_, P, stream))
+
+
+def adam(w, g, m, v, wh, n, lr, b1, b2, eps, step, wd, stream) -> None:
+    check(_adam(w, g, m, v, wh, n, lr, b1, b2, eps, step, wd, stream))
+
+
+def to_bf16(x, y, n, stream) -> None:
+    check(_to_bf16(x, y, n, stream))

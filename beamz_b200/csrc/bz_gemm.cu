@@ -1,0 +1,469 @@
+// Kernels of the learned surrogate (a Fourier neural operator over the design
+// density): a batched BF16 tensor-core GEMM with FP32 accumulation and fused
+// epilogues, the per-mode complex channel mixing of the spectral layers, and the
+// small elementwise kernels of training (GELU backward, pixel mean, Adam).
+// No counterpart in the reference, which has no learned surrogate.
+//
+// GEMM: C[b] = epilogue(alpha * op(A[b]) @ op(B[b])). Block tiles of BM x BN x 32
+// are staged through registers into padded shared memory with the reduction dim
+// (K) contiguous whatever the operands' layouts (80-byte rows keep ldmatrix free
+// of bank conflicts), double buffered, and multiplied by warps with
+// mma.sync.m16n8k16 (bf16 inputs, f32 accumulators). The epilogue adds an f32
+// term, row/column biases, applies GELU, and stores f32 and/or bf16, or
+// accumulates atomically (batch-reduced or split-K weight gradients).
+#include <cuda_bf16.h>
+
+#include "bz_internal.cuh"
+
+namespace bz {
+namespace {
+
+typedef __nv_bfloat16 bf16;
+constexpr int GBK = 32;
+constexpr int GPAD = 8;
+constexpr int GLD = GBK + GPAD;  // smem row length in bf16 elements (80 bytes)
+
+struct GemmP {
+  int M, N, K, batch, splitk, act, ta, tb, atomic;
+  const bf16* A;
+  long long lda, sa;
+  const bf16* B;
+  long long ldb, sb;
+  float alpha;
+  const float* cadd;
+  long long ldadd, sadd;
+  const float* bias_m;
+  const float* bias_n;
+  float* outf;
+  bf16* outh;
+  long long ldc, sc;
+  bf16* pre;
+  long long ldpre, spre;
+};
+
+__device__ __forceinline__ float gelu_f(float v) {
+  // tanh form of GELU
+  const float u = 0.7978845608028654f * (v + 0.044715f * v * v * v);
+  return 0.5f * v * (1.0f + tanhf(u));
+}
+
+__device__ __forceinline__ float gelu_grad(float v) {
+  const float u = 0.7978845608028654f * (v + 0.044715f * v * v * v);
+  const float t = tanhf(u);
+  const float du = 0.7978845608028654f * (1.0f + 3.0f * 0.044715f * v * v);
+  return 0.5f * (1.0f + t) + 0.5f * v * (1.0f - t * t) * du;
+}
+
+// 8 consecutive bf16 from p (elements idx .. idx+7 of a line with `lim` valid ones);
+// zero beyond the line or when !ok.
+__device__ __forceinline__ uint4 load8(const bf16* p, long long idx, long long lim, bool ok) {
+  uint4 r = make_uint4(0u, 0u, 0u, 0u);
+  if (!ok || idx >= lim) return r;
+  const bf16* q = p + idx;
+  if (idx + 8 <= lim && ((reinterpret_cast<uintptr_t>(q) & 15u) == 0u)) return __ldg(reinterpret_cast<const uint4*>(q));
+  unsigned short* h = reinterpret_cast<unsigned short*>(&r);
+  const unsigned short* s = reinterpret_cast<const unsigned short*>(q);
+  const int n = (int)min(8LL, lim - idx);
+  for (int i = 0; i < n; ++i) h[i] = s[i];
+  return r;
+}
+
+__device__ __forceinline__ void ldsm_x4(unsigned& r0, unsigned& r1, unsigned& r2, unsigned& r3, const bf16* p) {
+  const unsigned a = static_cast<unsigned>(__cvta_generic_to_shared(p));
+  asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0,%1,%2,%3}, [%4];\n"
+               : "=r"(r0), "=r"(r1), "=r"(r2), "=r"(r3)
+               : "r"(a));
+}
+
+__device__ __forceinline__ void mma_bf16(float* d, const unsigned* a, unsigned b0, unsigned b1) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+      "{%0,%1,%2,%3};\n"
+      : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+
+template <int BM, int BN, int WM, int WN>
+__global__ void __launch_bounds__(32 * WM * WN) gemm_bf16_kernel(GemmP p) {
+  constexpr int NT_ = 32 * WM * WN;
+  constexpr int TM = BM / WM, TN = BN / WN;  // warp tile
+  constexpr int MT = TM / 16, NT = TN / 8;
+  static_assert(NT % 2 == 0 && MT >= 1, "warp tile");
+  constexpr int CA = (BM * GBK / 8 + NT_ - 1) / NT_;  // 8-element chunks per thread
+  constexpr int CB = (BN * GBK / 8 + NT_ - 1) / NT_;
+  __shared__ __align__(16) bf16 As[2][BM][GLD];
+  __shared__ __align__(16) bf16 Bs[2][BN][GLD];
+
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int wm0 = (warp / WN) * TM, wn0 = (warp % WN) * TN;
+  const int bz = blockIdx.z / p.splitk, ks = blockIdx.z % p.splitk;
+  const int m0 = blockIdx.y * BM, n0 = blockIdx.x * BN;
+  const bf16* A = p.A + (long long)bz * p.sa;
+  const bf16* B = p.B + (long long)bz * p.sb;
+  const int ktiles = (p.K + GBK - 1) / GBK;
+  const int kper = (ktiles + p.splitk - 1) / p.splitk;
+  const int kt0 = ks * kper, kt1 = min(ktiles, kt0 + kper);
+
+  uint4 ra[CA], rb[CB];
+  auto gload = [&](int kt) {
+    const int k0 = kt * GBK;
+#pragma unroll
+    for (int c = 0; c < CA; ++c) {
+      const int ch = tid + c * NT_;
+      if (ch >= BM * GBK / 8) break;
+      if (!p.ta) {  // A[m][k], k contiguous
+        const int r = ch / (GBK / 8), kc = (ch % (GBK / 8)) * 8;
+        const int m = m0 + r;
+        ra[c] = load8(A + (long long)min(m, p.M - 1) * p.lda, k0 + kc, p.K, m < p.M);
+      } else {  // A stored [k][m], m contiguous
+        const int k = ch / (BM / 8), mc = (ch % (BM / 8)) * 8;
+        ra[c] = load8(A + (long long)min(k0 + k, p.K - 1) * p.lda, m0 + mc, p.M, k0 + k < p.K);
+      }
+    }
+#pragma unroll
+    for (int c = 0; c < CB; ++c) {
+      const int ch = tid + c * NT_;
+      if (ch >= BN * GBK / 8) break;
+      if (p.tb) {  // B stored [n][k], k contiguous
+        const int r = ch / (GBK / 8), kc = (ch % (GBK / 8)) * 8;
+        const int n = n0 + r;
+        rb[c] = load8(B + (long long)min(n, p.N - 1) * p.ldb, k0 + kc, p.K, n < p.N);
+      } else {  // B[k][n], n contiguous
+        const int k = ch / (BN / 8), nc = (ch % (BN / 8)) * 8;
+        rb[c] = load8(B + (long long)min(k0 + k, p.K - 1) * p.ldb, n0 + nc, p.N, k0 + k < p.K);
+      }
+    }
+  };
+  auto sstore = [&](int buf) {
+#pragma unroll
+    for (int c = 0; c < CA; ++c) {
+      const int ch = tid + c * NT_;
+      if (ch >= BM * GBK / 8) break;
+      if (!p.ta) {
+        const int r = ch / (GBK / 8), kc = (ch % (GBK / 8)) * 8;
+        *reinterpret_cast<uint4*>(&As[buf][r][kc]) = ra[c];
+      } else {
+        const int k = ch / (BM / 8), mc = (ch % (BM / 8)) * 8;
+        const bf16* h = reinterpret_cast<const bf16*>(&ra[c]);
+#pragma unroll
+        for (int i = 0; i < 8; ++i) As[buf][mc + i][k] = h[i];
+      }
+    }
+#pragma unroll
+    for (int c = 0; c < CB; ++c) {
+      const int ch = tid + c * NT_;
+      if (ch >= BN * GBK / 8) break;
+      if (p.tb) {
+        const int r = ch / (GBK / 8), kc = (ch % (GBK / 8)) * 8;
+        *reinterpret_cast<uint4*>(&Bs[buf][r][kc]) = rb[c];
+      } else {
+        const int k = ch / (BN / 8), nc = (ch % (BN / 8)) * 8;
+        const bf16* h = reinterpret_cast<const bf16*>(&rb[c]);
+#pragma unroll
+        for (int i = 0; i < 8; ++i) Bs[buf][nc + i][k] = h[i];
+      }
+    }
+  };
+
+  float acc[MT][NT][4];
+#pragma unroll
+  for (int i = 0; i < MT; ++i)
+#pragma unroll
+    for (int j = 0; j < NT; ++j)
+#pragma unroll
+      for (int e = 0; e < 4; ++e) acc[i][j][e] = 0.f;
+
+  if (kt0 < kt1) {
+    gload(kt0);
+    sstore(0);
+    __syncthreads();
+    for (int kt = kt0; kt < kt1; ++kt) {
+      const int buf = (kt - kt0) & 1;
+      if (kt + 1 < kt1) gload(kt + 1);
+#pragma unroll
+      for (int kk = 0; kk < GBK; kk += 16) {
+        unsigned af[MT][4], bfr[NT][2];
+#pragma unroll
+        for (int i = 0; i < MT; ++i)
+          ldsm_x4(af[i][0], af[i][1], af[i][2], af[i][3], &As[buf][wm0 + i * 16 + (lane & 15)][kk + (lane >> 4) * 8]);
+#pragma unroll
+        for (int j = 0; j < NT; j += 2)
+          ldsm_x4(bfr[j][0], bfr[j][1], bfr[j + 1][0], bfr[j + 1][1],
+                  &Bs[buf][wn0 + j * 8 + (lane & 7) + ((lane >> 4) << 3)][kk + ((lane >> 3) & 1) * 8]);
+#pragma unroll
+        for (int i = 0; i < MT; ++i)
+#pragma unroll
+          for (int j = 0; j < NT; ++j) mma_bf16(acc[i][j], af[i], bfr[j][0], bfr[j][1]);
+      }
+      if (kt + 1 < kt1) sstore(buf ^ 1);
+      __syncthreads();
+    }
+  }
+
+  // epilogue
+#pragma unroll
+  for (int i = 0; i < MT; ++i)
+#pragma unroll
+    for (int j = 0; j < NT; ++j)
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        const int m = m0 + wm0 + i * 16 + (lane >> 2) + (e >= 2 ? 8 : 0);
+        const int n = n0 + wn0 + j * 8 + (lane & 3) * 2 + (e & 1);
+        if (m >= p.M || n >= p.N) continue;
+        float v = p.alpha * acc[i][j][e];
+        if (p.cadd) v += p.cadd[(long long)bz * p.sadd + (long long)m * p.ldadd + n];
+        if (p.bias_m) v += p.bias_m[m];
+        if (p.bias_n) v += p.bias_n[n];
+        if (p.pre) p.pre[(long long)bz * p.spre + (long long)m * p.ldpre + n] = __float2bfloat16_rn(v);
+        if (p.act == 1) v = gelu_f(v);
+        const long long o = (long long)bz * p.sc + (long long)m * p.ldc + n;
+        if (p.outf) {
+          if (p.atomic) atomicAdd(p.outf + o, v); else p.outf[o] = v;
+        }
+        if (p.outh) p.outh[o] = __float2bfloat16_rn(v);
+      }
+}
+
+template <int BM, int BN, int WM, int WN>
+int launch_gemm(const GemmP& p, cudaStream_t st) {
+  dim3 grid((unsigned)ceil_div(p.N, BN), (unsigned)ceil_div(p.M, BM), (unsigned)(p.batch * p.splitk));
+  gemm_bf16_kernel<BM, BN, WM, WN><<<grid, 32 * WM * WN, 0, st>>>(p);
+  return check_launch("bz_gemm_bf16");
+}
+
+// ---- spectral channel mixing: O[b][o][k] = sum_c U[b][c][k] * W[k][c][o] (complex) ---
+// U, O: [B][C][n_modes][2] bf16 (re, im); W: [n_modes][Ci][Co][2] bf16.
+__global__ void spectral_fwd_kernel(const bf16* __restrict__ U, const bf16* __restrict__ W, bf16* __restrict__ O,
+                                    int B, int Ci, int Co, int nk) {
+  const int k = blockIdx.x;
+  const int o = threadIdx.x;  // Co threads
+  const bf16* w = W + (long long)k * Ci * Co * 2;
+  for (int b = blockIdx.y; b < B; b += gridDim.y) {
+    float re = 0.f, im = 0.f;
+    for (int c = 0; c < Ci; ++c) {
+      const long long ui = (((long long)b * Ci + c) * nk + k) * 2;
+      const float ur = __bfloat162float(U[ui]), uim = __bfloat162float(U[ui + 1]);
+      const float wr = __bfloat162float(w[(c * Co + o) * 2]), wi = __bfloat162float(w[(c * Co + o) * 2 + 1]);
+      re = fmaf(ur, wr, fmaf(-uim, wi, re));
+      im = fmaf(ur, wi, fmaf(uim, wr, im));
+    }
+    const long long oi = (((long long)b * Co + o) * nk + k) * 2;
+    O[oi] = __float2bfloat16_rn(re);
+    O[oi + 1] = __float2bfloat16_rn(im);
+  }
+}
+
+// dU[b][c][k] = sum_o dO[b][o][k] * conj(W[k][c][o]); thread per c.
+__global__ void spectral_bwd_u_kernel(const bf16* __restrict__ dO, const bf16* __restrict__ W, bf16* __restrict__ dU,
+                                      int B, int Ci, int Co, int nk) {
+  const int k = blockIdx.x;
+  const int c = threadIdx.x;
+  const bf16* w = W + (long long)k * Ci * Co * 2;
+  for (int b = blockIdx.y; b < B; b += gridDim.y) {
+    float re = 0.f, im = 0.f;
+    for (int o = 0; o < Co; ++o) {
+      const long long gi = (((long long)b * Co + o) * nk + k) * 2;
+      const float gr = __bfloat162float(dO[gi]), gim = __bfloat162float(dO[gi + 1]);
+      const float wr = __bfloat162float(w[(c * Co + o) * 2]), wi = __bfloat162float(w[(c * Co + o) * 2 + 1]);
+      re = fmaf(gr, wr, fmaf(gim, wi, re));
+      im = fmaf(gim, wr, fmaf(-gr, wi, im));
+    }
+    const long long ui = (((long long)b * Ci + c) * nk + k) * 2;
+    dU[ui] = __float2bfloat16_rn(re);
+    dU[ui + 1] = __float2bfloat16_rn(im);
+  }
+}
+
+// dW[k][c][o] += sum_b dO[b][o][k] * conj(U[b][c][k]) (f32); thread per (c, o).
+__global__ void spectral_bwd_w_kernel(const bf16* __restrict__ dO, const bf16* __restrict__ U, float* __restrict__ dW,
+                                      int B, int Ci, int Co, int nk) {
+  const int k = blockIdx.x;
+  for (int t = threadIdx.x; t < Ci * Co; t += blockDim.x) {
+    const int c = t / Co, o = t % Co;
+    float re = 0.f, im = 0.f;
+    for (int b = 0; b < B; ++b) {
+      const long long gi = (((long long)b * Co + o) * nk + k) * 2;
+      const long long ui = (((long long)b * Ci + c) * nk + k) * 2;
+      const float gr = __bfloat162float(dO[gi]), gim = __bfloat162float(dO[gi + 1]);
+      const float ur = __bfloat162float(U[ui]), uim = __bfloat162float(U[ui + 1]);
+      re = fmaf(gr, ur, fmaf(gim, uim, re));
+      im = fmaf(gim, ur, fmaf(-gr, uim, im));
+    }
+    float* d = dW + (((long long)k * Ci + c) * Co + o) * 2;
+    d[0] += re;
+    d[1] += im;
+  }
+}
+
+__global__ void gelu_bwd_kernel(const bf16* __restrict__ dy, const bf16* __restrict__ pre, bf16* __restrict__ dx,
+                                long long n) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    dx[i] = __float2bfloat16_rn(__bfloat162float(dy[i]) * gelu_grad(__bfloat162float(pre[i])));
+}
+
+// out[r] = scale * sum_p x[r][p] over rows r of length P (bf16 in, f32 out): one warp per row.
+__global__ void row_mean_kernel(const bf16* __restrict__ x, float* __restrict__ out, long long rows, int P,
+                                float scale) {
+  const long long r = blockIdx.x * (long long)(blockDim.x / 32) + (threadIdx.x >> 5);
+  if (r >= rows) return;
+  const int lane = threadIdx.x & 31;
+  float s = 0.f;
+  for (int p = lane; p < P; p += 32) s += __bfloat162float(x[r * P + p]);
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  if (lane == 0) out[r] = s * scale;
+}
+
+// Sum over rows: out[c] += sum_{b} sum_p x[b][c][p] (bf16 in, f32 out); block per (c).
+__global__ void chan_sum_kernel(const bf16* __restrict__ x, float* __restrict__ out, int B, int C, int P) {
+  const int c = blockIdx.x;
+  float s = 0.f;
+  for (int b = 0; b < B; ++b)
+    for (int p = threadIdx.x; p < P; p += blockDim.x) s += __bfloat162float(x[((long long)b * C + c) * P + p]);
+  __shared__ float red[32];
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    s = threadIdx.x < (int)(blockDim.x >> 5) ? red[threadIdx.x] : 0.f;
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if (threadIdx.x == 0) out[c] += s;
+  }
+}
+
+// x[r][p] = g[r] * scale (broadcast of a per-row gradient), bf16 out.
+__global__ void row_broadcast_kernel(const float* __restrict__ g, bf16* __restrict__ x, long long rows, int P,
+                                     float scale) {
+  const long long n = rows * P;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    x[i] = __float2bfloat16_rn(g[i / P] * scale);
+}
+
+// Adam on f32 master weights; refreshes the bf16 copy used by the kernels.
+__global__ void adam_kernel(float* __restrict__ w, const float* __restrict__ g, float* __restrict__ m,
+                            float* __restrict__ v, bf16* __restrict__ wh, long long n, float lr, float b1, float b2,
+                            float eps, float c1, float c2, float wd) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const float gi = g[i] + wd * w[i];
+    const float mi = b1 * m[i] + (1.f - b1) * gi;
+    const float vi = b2 * v[i] + (1.f - b2) * gi * gi;
+    m[i] = mi;
+    v[i] = vi;
+    const float wn = w[i] - lr * (mi / c1) / (sqrtf(vi / c2) + eps);
+    w[i] = wn;
+    if (wh) wh[i] = __float2bfloat16_rn(wn);
+  }
+}
+
+__global__ void to_bf16_kernel(const float* __restrict__ x, bf16* __restrict__ y, long long n) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    y[i] = __float2bfloat16_rn(x[i]);
+}
+
+unsigned grid_for(long long n, int threads) {
+  const long long b = (n + threads - 1) / threads;
+  return (unsigned)(b < 148LL * 32 ? (b < 1 ? 1 : b) : 148LL * 32);
+}
+
+}  // namespace
+}  // namespace bz
+
+extern "C" int bz_gemm_bf16(const bz_gemm* g, void* stream) {
+  BZ_REQUIRE(g != nullptr, "bz_gemm_bf16: NULL arguments");
+  BZ_REQUIRE(g->M >= 0 && g->N >= 0 && g->K >= 0 && g->batch >= 1 && g->splitk >= 1,
+             "bz_gemm_bf16: bad sizes M=%d N=%d K=%d batch=%d splitk=%d", g->M, g->N, g->K, g->batch, g->splitk);
+  BZ_REQUIRE(g->A && g->B, "bz_gemm_bf16: NULL operand");
+  BZ_REQUIRE(g->outf || g->outh, "bz_gemm_bf16: no output");
+  BZ_REQUIRE(!(g->atomic || g->splitk > 1) || (g->outf && !g->outh && !g->cadd && !g->bias_m && !g->bias_n &&
+                                                !g->pre && g->act == 0),
+             "bz_gemm_bf16: atomic/split-K output takes a plain f32 product only");
+  BZ_REQUIRE(g->splitk == 1 || g->atomic, "bz_gemm_bf16: split-K needs atomic accumulation");
+  BZ_REQUIRE(g->act == 0 || g->act == 1, "bz_gemm_bf16: unknown activation %d", g->act);
+  BZ_REQUIRE((long long)g->batch * g->splitk <= 65535, "bz_gemm_bf16: batch x splitk above 65535");
+  if (g->M == 0 || g->N == 0) return BZ_OK;
+  bz::GemmP p;
+  p.M = g->M; p.N = g->N; p.K = g->K; p.batch = g->batch; p.splitk = g->splitk; p.act = g->act;
+  p.ta = g->ta; p.tb = g->tb; p.atomic = g->atomic;
+  p.A = (const bz::bf16*)g->A; p.lda = g->lda; p.sa = g->sa;
+  p.B = (const bz::bf16*)g->B; p.ldb = g->ldb; p.sb = g->sb;
+  p.alpha = g->alpha;
+  p.cadd = g->cadd; p.ldadd = g->ldadd; p.sadd = g->sadd;
+  p.bias_m = g->bias_m; p.bias_n = g->bias_n;
+  p.outf = g->outf; p.outh = (bz::bf16*)g->outh; p.ldc = g->ldc; p.sc = g->sc;
+  p.pre = (bz::bf16*)g->pre; p.ldpre = g->ldpre; p.spre = g->spre;
+  cudaStream_t st = bz::as_stream(stream);
+  if (g->N <= 32) return bz::launch_gemm<128, 32, 4, 1>(p, st);
+  if (g->M <= 32) return bz::launch_gemm<32, 128, 1, 4>(p, st);
+  return bz::launch_gemm<128, 128, 2, 4>(p, st);
+}
+
+extern "C" int bz_spectral_mix(const void* U, const void* W, void* O, int32_t B, int32_t ci, int32_t co,
+                               int32_t n_modes, void* stream) {
+  BZ_REQUIRE(U && W && O, "bz_spectral_mix: NULL buffer");
+  BZ_REQUIRE(B >= 1 && ci >= 1 && co >= 1 && co <= 1024 && n_modes >= 1, "bz_spectral_mix: bad sizes");
+  dim3 grid((unsigned)n_modes, (unsigned)(B < 64 ? B : 64));
+  bz::spectral_fwd_kernel<<<grid, co, 0, bz::as_stream(stream)>>>((const bz::bf16*)U, (const bz::bf16*)W,
+                                                                     (bz::bf16*)O, B, ci, co, n_modes);
+  return bz::check_launch("bz_spectral_mix");
+}
+
+extern "C" int bz_spectral_mix_bwd(const void* dO, const void* U, const void* W, void* dU, float* dW, int32_t B,
+                                   int32_t ci, int32_t co, int32_t n_modes, void* stream) {
+  BZ_REQUIRE(dO && U && W && dU && dW, "bz_spectral_mix_bwd: NULL buffer");
+  BZ_REQUIRE(B >= 1 && ci >= 1 && ci <= 1024 && co >= 1 && n_modes >= 1, "bz_spectral_mix_bwd: bad sizes");
+  cudaStream_t st = bz::as_stream(stream);
+  dim3 grid((unsigned)n_modes, (unsigned)(B < 64 ? B : 64));
+  bz::spectral_bwd_u_kernel<<<grid, ci, 0, st>>>((const bz::bf16*)dO, (const bz::bf16*)W, (bz::bf16*)dU, B, ci, co,
+                                                 n_modes);
+  int rc = bz::check_launch("bz_spectral_mix_bwd");
+  if (rc != BZ_OK) return rc;
+  bz::spectral_bwd_w_kernel<<<(unsigned)n_modes, 256, 0, st>>>((const bz::bf16*)dO, (const bz::bf16*)U, dW, B, ci,
+                                                               co, n_modes);
+  return bz::check_launch("bz_spectral_mix_bwd");
+}
+
+extern "C" int bz_gelu_bwd(const void* dy, const void* pre, void* dx, int64_t n, void* stream) {
+  BZ_REQUIRE(dy && pre && dx && n >= 0, "bz_gelu_bwd: bad arguments");
+  if (n == 0) return BZ_OK;
+  bz::gelu_bwd_kernel<<<bz::grid_for(n, 256), 256, 0, bz::as_stream(stream)>>>(
+      (const bz::bf16*)dy, (const bz::bf16*)pre, (bz::bf16*)dx, n);
+  return bz::check_launch("bz_gelu_bwd");
+}
+
+extern "C" int bz_row_mean(const void* x, float* out, int64_t rows, int32_t P, float scale, void* stream) {
+  BZ_REQUIRE(x && out && rows >= 0 && P >= 1, "bz_row_mean: bad arguments");
+  if (rows == 0) return BZ_OK;
+  bz::row_mean_kernel<<<(unsigned)bz::ceil_div(rows, 8), 256, 0, bz::as_stream(stream)>>>((const bz::bf16*)x, out,
+                                                                                        rows, P, scale);
+  return bz::check_launch("bz_row_mean");
+}
+
+extern "C" int bz_row_broadcast(const float* g, void* x, int64_t rows, int32_t P, float scale, void* stream) {
+  BZ_REQUIRE(g && x && rows >= 0 && P >= 1, "bz_row_broadcast: bad arguments");
+  if (rows == 0) return BZ_OK;
+  bz::row_broadcast_kernel<<<bz::grid_for(rows * P, 256), 256, 0, bz::as_stream(stream)>>>(g, (bz::bf16*)x, rows, P,
+                                                                                          scale);
+  return bz::check_launch("bz_row_broadcast");
+}
+
+extern "C" int bz_chan_sum(const void* x, float* out, int32_t B, int32_t C, int32_t P, void* stream) {
+  BZ_REQUIRE(x && out && B >= 1 && C >= 1 && P >= 1, "bz_chan_sum: bad arguments");
+  bz::chan_sum_kernel<<<(unsigned)C, 256, 0, bz::as_stream(stream)>>>((const bz::bf16*)x, out, B, C, P);
+  return bz::check_launch("bz_chan_sum");
+}
+
+extern "C" int bz_adam(float* w, const float* g, float* m, float* v, void* wh, int64_t n, float lr, float b1,
+                       float b2, float eps, int32_t step, float weight_decay, void* stream) {
+  BZ_REQUIRE(w && g && m && v && n >= 0 && step >= 1, "bz_adam: bad arguments");
+  if (n == 0) return BZ_OK;
+  const float c1 = 1.f - powf(b1, (float)step), c2 = 1.f - powf(b2, (float)step);
+  bz::adam_kernel<<<bz::grid_for(n, 256), 256, 0, bz::as_stream(stream)>>>(w, g, m, v, (bz::bf16*)wh, n, lr, b1, b2,
+                                                                          eps, c1, c2, weight_decay);
+  return bz::check_launch("bz_adam");
+}
+
+extern "C" int bz_to_bf16(const float* x, void* y, int64_t n, void* stream) {
+  BZ_REQUIRE(x && y && n >= 0, "bz_to_bf16: bad arguments");
+  if (n == 0) return BZ_OK;
+  bz::to_bf16_kernel<<<bz::grid_for(n, 256), 256, 0, bz::as_stream(stream)>>>(x, (bz::bf16*)y, n);
+  return bz::check_launch("bz_to_bf16");
+}

@@ -381,6 +381,63 @@ int bz_rasterize3d(int32_t nx, int32_t ny, int32_t nz, int32_t n_zs, const doubl
                    int32_t n_pml, const double* pml_table, const double* prof_z, double sigma_factor_z, double dx,
                    double eps0, double mu0, double* eps, double* mu, double* sigma, void* stream);
 
+/* ---- learned surrogate kernels ------------------------------------------------
+ * No counterpart in the reference (it has no learned surrogate). A Fourier neural
+ * operator maps a design density to transmissions; its layers are built from these
+ * kernels: bf16 operands and activations, f32 accumulation. */
+
+/* C[b] = epilogue(alpha * op(A[b]) @ op(B[b])) for b < batch, M x N x K:
+ * op(A)[m][k] = A[m*lda + k] (ta = 0) or A[k*lda + m] (ta = 1); op(B)[k][n] =
+ * B[k*ldb + n] (tb = 0) or B[n*ldb + k] (tb = 1); sa/sb/sc/sadd/spre are batch
+ * strides in elements (0 shares an operand across the batch). Epilogue, in order:
+ * + cadd[b][m][n] (f32, optional), + bias_m[m], + bias_n[n] (f32, optional), a copy
+ * to pre (bf16, optional), act (0 none, 1 GELU tanh form), then store to outf (f32)
+ * and/or outh (bf16). atomic = 1 adds alpha*product into outf (f32 only, no other
+ * epilogue term), which with sc = 0 reduces over the batch; splitk > 1 splits K
+ * across blocks and needs atomic. */
+typedef struct bz_gemm {
+  int32_t M, N, K, batch, splitk, act;
+  int32_t ta, tb, atomic, reserved;
+  const void* A;
+  int64_t lda, sa;
+  const void* B;
+  int64_t ldb, sb;
+  float alpha, reserved2;
+  const float* cadd;
+  int64_t ldadd, sadd;
+  const float* bias_m;
+  const float* bias_n;
+  float* outf;
+  void* outh;
+  int64_t ldc, sc;
+  void* pre;
+  int64_t ldpre, spre;
+} bz_gemm;
+
+int bz_gemm_bf16(const bz_gemm* g, void* stream);
+
+/* Spectral channel mixing of one Fourier layer, per mode k < n_modes:
+ * O[b][o][k] = sum_c U[b][c][k] * W[k][c][o] (complex, (re, im) pairs, bf16). */
+int bz_spectral_mix(const void* U, const void* W, void* O, int32_t B, int32_t ci, int32_t co, int32_t n_modes,
+                    void* stream);
+/* Its backward: dU = sum_o dO * conj(W); dW (f32, accumulated) += sum_b dO * conj(U). */
+int bz_spectral_mix_bwd(const void* dO, const void* U, const void* W, void* dU, float* dW, int32_t B, int32_t ci,
+                        int32_t co, int32_t n_modes, void* stream);
+/* dx = dy * GELU'(pre) (bf16). */
+int bz_gelu_bwd(const void* dy, const void* pre, void* dx, int64_t n, void* stream);
+/* out[r] = scale * sum_p x[r][p] (bf16 rows of length P, f32 out). */
+int bz_row_mean(const void* x, float* out, int64_t rows, int32_t P, float scale, void* stream);
+/* x[r][p] = scale * g[r] (bf16 out). */
+int bz_row_broadcast(const float* g, void* x, int64_t rows, int32_t P, float scale, void* stream);
+/* out[c] += sum_b sum_p x[b][c][p] (bf16 [B][C][P], f32 out). */
+int bz_chan_sum(const void* x, float* out, int32_t B, int32_t C, int32_t P, void* stream);
+/* One Adam step (bias-corrected, decoupled weight decay folded into the gradient) on
+ * f32 master weights w with moments m, v; refreshes the bf16 copy wh when non-NULL. */
+int bz_adam(float* w, const float* g, float* m, float* v, void* wh, int64_t n, float lr, float b1, float b2,
+            float eps, int32_t step, float weight_decay, void* stream);
+/* y = bf16(x). */
+int bz_to_bf16(const float* x, void* y, int64_t n, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,0 +1,115 @@
+"""Surrogate kernels on the GPU.
+
+* bz_gemm_bf16 against an f32 matmul of the same bf16 operands: relative L2 error
+  <= 1e-5 for f32 outputs (accumulation order only), <= 8e-3 for bf16 outputs;
+  every transpose combination, batch sharing, epilogue terms and split-K atomics.
+* The FNO (bf16 activations and weights, f32 accumulation) against the float64
+  oracle (oracle/fno_ref.py) with the same master weights: outputs within 3e-2
+  relative L2; parameter and input gradients (explicit backward) within 6e-2
+  relative L2 of the oracle's autograd.
+"""
+import numpy as np
+import pytest
+import torch
+
+from oracle import fno_ref
+
+pytestmark = pytest.mark.gpu
+
+
+def rel(a, b):
+    a, b = torch.as_tensor(a).double().cpu(), torch.as_tensor(b).double().cpu()
+    return float((a - b).norm() / max(float(b.norm()), 1e-300))
+
+
+@pytest.mark.parametrize("ta,tb", [(0, 0), (0, 1), (1, 0), (1, 1)])
+@pytest.mark.parametrize("M,N,K", [(37, 45, 70), (200, 30, 64), (24, 300, 19), (130, 260, 96)])
+def test_gemm_matches_f32_matmul(bz, ta, tb, M, N, K):
+    from beamz_b200 import _native as nat
+
+    g = torch.Generator().manual_seed(M * 7 + N + K)
+    batch = 3
+    A = torch.randn(batch, M, K, generator=g).to(torch.bfloat16)
+    B = torch.randn(batch, K, N, generator=g).to(torch.bfloat16)
+    add = torch.randn(batch, M, N, generator=g)
+    bm, bn = torch.randn(M, generator=g), torch.randn(N, generator=g)
+    want = torch.bmm(A.float(), B.float()) * 0.5 + add + bm[None, :, None] + bn[None, None, :]
+    dev = "cuda"
+    Ad = (A.transpose(1, 2) if ta else A).contiguous().to(dev)
+    Bd = (B.transpose(1, 2) if tb else B).contiguous().to(dev)
+    outf = torch.empty(batch, M, N, device=dev)
+    outh = torch.empty(batch, M, N, device=dev, dtype=torch.bfloat16)
+    pre = torch.empty_like(outh)
+    p = nat.Gemm()
+    p.M, p.N, p.K, p.batch, p.splitk, p.act, p.ta, p.tb, p.atomic = M, N, K, batch, 1, 0, ta, tb, 0
+    p.A, p.lda, p.sa = Ad.data_ptr(), (M if ta else K), M * K
+    p.B, p.ldb, p.sb = Bd.data_ptr(), (K if tb else N), K * N
+    p.alpha = 0.5
+    addd, bmd, bnd = add.to(dev), bm.to(dev), bn.to(dev)
+    p.cadd, p.ldadd, p.sadd = addd.data_ptr(), N, M * N
+    p.bias_m, p.bias_n = bmd.data_ptr(), bnd.data_ptr()
+    p.outf, p.outh, p.ldc, p.sc = outf.data_ptr(), outh.data_ptr(), N, M * N
+    p.pre, p.ldpre, p.spre = pre.data_ptr(), N, M * N
+    nat.gemm(p, torch.cuda.current_stream().cuda_stream)
+    torch.cuda.synchronize()
+    assert rel(outf, want) <= 1e-5
+    assert rel(outh.float(), want) <= 8e-3
+    # GELU epilogue and split-K atomic accumulation over a shared output
+    p.act = 1
+    nat.gemm(p, torch.cuda.current_stream().cuda_stream)
+    assert rel(outf, fno_ref.gelu(want.double())) <= 1e-5
+    assert rel(pre.float(), want) <= 8e-3
+    acc = torch.zeros(M, N, device=dev)
+    q = nat.Gemm.from_buffer_copy(p)
+    q.act, q.cadd, q.bias_m, q.bias_n, q.outh, q.pre = 0, None, None, None, None, None
+    q.alpha, q.atomic, q.splitk, q.outf, q.sc = 1.0, 1, 3, acc.data_ptr(), 0
+    nat.gemm(q, torch.cuda.current_stream().cuda_stream)
+    assert rel(acc, torch.bmm(A.float(), B.float()).sum(0)) <= 1e-5
+
+
+def _small_fno(bz, seed=0):
+    from beamz_b200.surrogate.fno import FNO2d
+
+    return FNO2d(n=24, width=8, modes=4, layers=3, head=16, n_out=5, seed=seed)
+
+
+def _oracle_params(net):
+    return {k: q.w.detach().double().cpu().clone().requires_grad_(True) for k, q in net.params.items()}
+
+
+def test_fno_forward_and_gradients_match_float64_oracle(bz):
+    net = _small_fno(bz)
+    g = torch.Generator().manual_seed(3)
+    rho = torch.rand(4, 24, 24, generator=g, dtype=torch.float64)
+    target = torch.rand(4, 5, generator=g, dtype=torch.float64)
+    out = net.forward(rho.cuda(), keep=True)
+    params = _oracle_params(net)
+    rho_r = rho.clone().requires_grad_(True)
+    ref = fno_ref.forward(params, rho_r, 24, 4, 3)
+    assert rel(out, ref.detach()) <= 3e-2
+    loss = ((ref - target) ** 2).sum()
+    loss.backward()
+    d_out = 2 * (ref.detach() - target)
+    net.zero_grad()
+    d_rho = net.backward(d_out.float().cuda(), want_input_grad=True)
+    for k, q in net.params.items():
+        assert rel(q.g, params[k].grad) <= 6e-2, (k, rel(q.g, params[k].grad))
+    assert rel(d_rho, rho_r.grad) <= 6e-2
+
+
+def test_fno_training_reduces_loss(bz):
+    """A few hundred Adam steps on a smooth functional of the density."""
+    net = _small_fno(bz, seed=1)
+    g = torch.Generator().manual_seed(4)
+    rho = torch.rand(64, 24, 24, generator=g)
+    w = torch.linspace(0.2, 1.0, 5)
+    target = (rho.mean(dim=(1, 2))[:, None] * w[None, :] + 0.1 * rho[:, :12].mean(dim=(1, 2))[:, None]).cuda()
+    losses = []
+    for it in range(300):
+        out = net.forward(rho.cuda(), keep=True)
+        err = out - target
+        losses.append(float((err ** 2).mean()))
+        net.zero_grad()
+        net.backward(2 * err / err.numel())
+        net.adam_step(lr=3e-3)
+    assert losses[-1] < 0.05 * losses[0], (losses[0], losses[-1])

@@ -100,3 +100,28 @@ def test_oracle_3d_matches_reference_run(bz, golden):
             np.testing.assert_array_equal(rec["fields"][k], g[f"m{i}_{k}"])
         np.testing.assert_array_equal(rec["t"], g[f"m{i}_t"])
         np.testing.assert_array_equal(rec["power"], g[f"m{i}_power"])
+
+
+def test_fno_oracle_spectral_round_trip():
+    """The oracle's truncated DFT followed by its inverse reproduces a field made of
+    the kept modes (pins the basis, the Hermitian weights and the 1/P scale)."""
+    import torch
+
+    from oracle import fno_ref
+
+    n, m = 16, 4
+    cos, sin, w = fno_ref.bases(n, m)
+    rng = np.random.default_rng(0)
+    a = rng.standard_normal(cos.shape[1])
+    b = rng.standard_normal(cos.shape[1])
+    KX = np.tile(np.arange(m), 2 * m)
+    KY = np.repeat(np.concatenate([np.arange(m), np.arange(n - m, n)]), m)
+    # kx = 0 modes come in +ky/-ky pairs (each carries half), except ky = 0 (alone) and
+    # ky = -m, whose partner +m is not kept: leave that one out of the test field
+    amp = np.where(KX == 0, np.where(KY == 0, 1.0, 0.5), 1.0)
+    amp[(KX == 0) & (KY == n - m)] = 0.0
+    v = (cos.numpy() @ (a * amp)) - (sin.numpy() @ (b * amp))
+    V = torch.as_tensor(v)
+    ur, ui = V @ cos, -(V @ sin)
+    back = (ur * w) @ cos.T - (ui * w) @ sin.T
+    np.testing.assert_allclose(back.numpy(), v, rtol=1e-9, atol=1e-9 * np.abs(v).max())
