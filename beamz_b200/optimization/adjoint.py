@@ -7,10 +7,11 @@ by overlapping a forward field history with a separately driven adjoint run
 exact reverse-mode derivative of the discrete update (``bz_adjoint_step2d``), so it
 agrees with finite differences of the same simulation.
 
-Objective: the power in a target mode at one frequency, measured on a line
-monitor, ``J = |a|^2`` with ``a = sum_p w_p E_w(p)``, ``E_w(p) = sum_n E_{n+1}(p)
-exp(-i w (n+1) dt) dt`` (the DFT convention of the frequency-domain monitors) and
-``w_p = conj(m_p) ds`` for a mode profile m on the monitor cells.
+Objective: the power in a target mode, measured on a line monitor at one or more
+frequencies, ``J = sum_f c_f |a_f|^2`` with ``a_f = sum_p w_fp E_f(p)``,
+``E_f(p) = sum_n E_{n+1}(p) exp(-i w_f (n+1) dt) dt`` (the DFT convention of the
+frequency-domain monitors) and ``w_fp = conj(m_f(p)) ds`` for the mode profile m_f of
+each frequency on the monitor cells (c_f = 1 by default).
 
 Memory/compute trade: forward states are checkpointed every K steps; each K-step
 segment is recomputed once during the backward sweep with the design-region
@@ -40,13 +41,15 @@ class AdjointFDTD2D:
     dx, dt, n_steps : grid spacing, time step and number of steps (dy = dx).
     sources : beamz_b200 sources (GaussianSource / ModeSource) driving the forward run.
     monitor : a 2D line Monitor; its cells carry the objective.
-    mode_profile : complex values m_p on the monitor's cells (length = its point count).
-    frequency : objective frequency in Hz.
+    mode_profile : complex values m_p on the monitor's cells (length = its point count),
+        or one row per frequency.
+    frequency : objective frequency in Hz, or a sequence of them.
+    weights : optional c_f per frequency.
     region : (y0, x0, h, w) cell box of the design region.
     """
 
     def __init__(self, eps_base, sigma, dx, dt, n_steps, sources, monitor, mode_profile, frequency, region, *,
-                 n_designs=1, precision="fp32", checkpoint_every=500):
+                 n_designs=1, precision="fp32", checkpoint_every=500, weights=None):
         self.eps_base = np.asarray(eps_base, dtype=np.float64)
         self.sigma = np.asarray(sigma, dtype=np.float64)
         self.ny, self.nx = self.eps_base.shape
@@ -59,16 +62,20 @@ class AdjointFDTD2D:
         self.B = int(n_designs)
         self.precision = precision
         self.K = int(checkpoint_every)
-        self.frequency = float(frequency)
-        mon = Monitor(start=monitor.start, end=monitor.end, frequencies=[self.frequency], record_fields=False,
+        self.freqs = np.atleast_1d(np.asarray(frequency, dtype=float))
+        self.frequency = float(self.freqs[0])
+        nf = len(self.freqs)
+        self.c_f = np.ones(nf) if weights is None else np.asarray(weights, dtype=float).reshape(nf)
+        mon = Monitor(start=monitor.start, end=monitor.end, frequencies=list(self.freqs), record_fields=False,
                       accumulate_power=False)
         self.monitor = mon
-        self.mode = np.asarray(mode_profile, dtype=complex)
+        mode = np.asarray(mode_profile, dtype=complex)
+        self.mode = np.broadcast_to(mode if mode.ndim == 2 else mode[None], (nf, mode.shape[-1])).copy()
         pts = mon.get_grid_points_2d(dx, dx)
-        if len(pts) != len(self.mode):
-            raise ValueError(f"mode profile has {len(self.mode)} values, the monitor {len(pts)} cells")
+        if len(pts) != self.mode.shape[1]:
+            raise ValueError(f"mode profile has {self.mode.shape[1]} values, the monitor {len(pts)} cells")
         self.ds = dx
-        self.wp = np.conj(self.mode) * self.ds
+        self.wp = np.conj(self.mode) * self.ds  # [F][P]
         self.mon_cells = [(int(y), int(x)) for x, y in pts]
         src_ops = compile_sources(self.sources, (self.ny, self.nx), (dx, dx), self.n_steps)
         for c in src_ops.cell:
@@ -87,13 +94,22 @@ class AdjointFDTD2D:
         return full, eps_region
 
     def _build(self, eps_region):
-        full, er = self._eps_full(eps_region)
         if self.engine is None:
+            full, er = self._eps_full(eps_region)
             self.engine = Engine2D(full, self.sigma, self.dx, self.dx, self.dt, self.n_steps, self.sources,
                                    [self.monitor], precision=self.precision, n_comp=1, n_designs=self.B,
                                    record=False, use_graphs=True)
+            dev = self.engine.dev
+            self._eps_t = torch.as_tensor(self.eps_base).to(dev)
+            self._sigma_t = torch.as_tensor(self.sigma).to(dev).expand(self.B, self.ny, self.nx).contiguous()
         else:
-            self.engine.set_material(full, self.sigma)
+            # only the design region crosses to the device
+            er = np.asarray(eps_region, dtype=np.float64).reshape(self.B, self.region[2], self.region[3])
+            y0, x0, h, w = self.region
+            full_t = self._eps_t.expand(self.B, self.ny, self.nx).clone()
+            full_t[:, y0:y0 + h, x0:x0 + w] = torch.as_tensor(er).to(full_t.device)
+            self.engine.h2d_bytes += er.nbytes
+            self.engine.set_material_tensors(full_t, self._sigma_t)
         self.eps_region = er
 
     # ---- forward ---------------------------------------------------------------
@@ -109,37 +125,40 @@ class AdjointFDTD2D:
                 cur = eng.cur
                 self.ckpt.append(tuple(b[cur].clone() for b in (eng.ez, eng.hx, eng.hy)))
             eng.run_steps(min(self.K, self.n_steps - s * self.K))
-        d = eng.dft_fields()  # [B][1][P][1][5]
-        ew = d[:, 0, :, 0, 0]  # E_w at the monitor cells, [B][P]
-        self.a = ew @ self.wp
-        return np.abs(self.a) ** 2
+        d = eng.dft_fields()  # [B][1][P][F][5]
+        ew = d[:, 0, :, :, 0]  # E_f at the monitor cells, [B][P][F]
+        self.a = np.einsum("bpf,fp->bf", ew, self.wp)
+        self.power = np.abs(self.a) ** 2  # [B][F]
+        return self.power @ self.c_f
 
     # ---- backward -----------------------------------------------------------------
     def _adjoint_ops(self):
         """Operations preparing dJ/dEt from dJ/dE: the forward sources' zeroing mask and
-        the objective term Re(alpha_p phi_n), phi_n = exp(-i w (n+1) dt) dt."""
+        the objective terms sum_f Re(alpha_fp phi_f(n)), phi_f(n) = exp(-i w_f (n+1) dt) dt."""
         fo = self._fwd_ops
         M = {}
         for c, m in zip(fo.cell, fo.mul):
             M[int(c)] = M.get(int(c), 1.0) * m  # composite multiplier of each cell
-        alpha = 2.0 * np.conj(self.a)[:, None] * self.wp[None, :]  # [B][P]
+        nf = len(self.freqs)
+        alpha = 2.0 * (self.c_f[None, :] * np.conj(self.a))[:, :, None] * self.wp[None]  # [B][F][P]
         per_cell = {}
         for p, (y, x) in enumerate(self.mon_cells):
             if 0 <= x < self.nx and 0 <= y < self.ny:
                 c = y * self.nx + x
-                per_cell[c] = per_cell.get(c, 0) + alpha[:, p]
+                per_cell[c] = per_cell.get(c, 0) + alpha[:, :, p]
         cells = sorted(set(per_cell) | {c for c, m in M.items() if m != 1.0})
         n = np.arange(self.n_steps, dtype=np.float64)
-        phi = np.exp(-1j * 2 * np.pi * self.frequency * (n + 1.0) * self.dt) * self.dt
-        signals = np.stack([phi.real, phi.imag])
+        phi = np.exp(-1j * 2 * np.pi * self.freqs[:, None] * (n[None, :] + 1.0) * self.dt) * self.dt  # [F][n]
+        signals = np.stack([phi.real, phi.imag], axis=1).reshape(2 * nf, self.n_steps)
         op_cell, op_mul, op_sig, w_cols = [], [], [], []
         for c in cells:
             m = M.get(c, 1.0)
-            a = per_cell.get(c, np.zeros(self.B, dtype=complex))
-            op_cell += [c, c]
-            op_mul += [m, 1.0]
-            op_sig += [0, 1]
-            w_cols += [m * a.real, -m * a.imag]
+            a = per_cell.get(c, np.zeros((self.B, nf), dtype=complex))
+            for f in range(nf):  # v <- m*v + m*Re(alpha_0 phi_0), then + m*Re(alpha_f phi_f)
+                op_cell += [c, c]
+                op_mul += [m if f == 0 else 1.0, 1.0]
+                op_sig += [2 * f, 2 * f + 1]
+                w_cols += [m * a[:, f].real, -m * a[:, f].imag]
         weight = np.stack(w_cols, axis=1) if w_cols else np.zeros((self.B, 0))  # [B][n_ops]
         # The seed is ~|a| dx dt (tiny in SI units); the adjoint is linear, so each
         # design's seed is scaled to O(1) (keeps float32 adjoint fields in range) and

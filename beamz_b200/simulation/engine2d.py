@@ -94,9 +94,16 @@ class Engine2D:
         shape = (self.n_mat, self.ny, self.nx)
         eps_r = np.ascontiguousarray(np.broadcast_to(np.asarray(eps_r, dtype=np.float64), shape))
         sigma = np.ascontiguousarray(np.broadcast_to(np.asarray(sigma, dtype=np.float64), shape))
-        te = torch.as_tensor(eps_r).to(self.dev)
-        ts = torch.as_tensor(sigma).to(self.dev)
         self.h2d_bytes += eps_r.nbytes + sigma.nbytes
+        self.set_material_tensors(torch.as_tensor(eps_r).to(self.dev), torch.as_tensor(sigma).to(self.dev))
+
+    def set_material_tensors(self, eps_r: torch.Tensor, sigma: torch.Tensor):
+        """As set_material, from float64 device tensors of shape [n_mat][ny][nx]."""
+        shape = (self.n_mat, self.ny, self.nx)
+        if tuple(eps_r.shape) != shape or tuple(sigma.shape) != shape:
+            raise ValueError(f"material tensors must have shape {shape}")
+        te = eps_r.to(self.dev, torch.float64).contiguous()
+        ts = sigma.to(self.dev, torch.float64).contiguous()
         nat.prepare_coeffs(te.data_ptr(), ts.data_ptr(), self.n_mat * self.ny, self.nx, self.pitch, self.bz_dtype,
                            self.dt, EPS_0, self.dy, self.ce.data_ptr(), self.loss.data_ptr(), self._stream())
         torch.cuda.current_stream().synchronize()

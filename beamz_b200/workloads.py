@@ -120,14 +120,19 @@ def soi_mmi_3d(nx=600, ny=300, nz=150, dx=0.02 * µm, n_steps=8000, pml=16, grid
 
 
 def topo_2d(n_designs=64, nx=600, ny=400, dx=0.02 * µm, n_steps=8000, pml=20, region_cells=120, seed=1234,
-            mode_points=None):
+            mode_points=None, wavelengths=None):
     """Batched topology-optimisation problem: B densities (120x120 cells, uniform in
     [0, 1] then Gaussian-smoothed with sigma = 3 cells, seeds seed+b) mapped to
     eps = 2.085 + rho * (12.25 - 2.085), centred in a 600x400 grid between 500 nm input
     and output Si waveguides in SiO2; CW mode source at 1.55 um; the objective is the
     power in the output guide's fundamental slab mode at 1.55 um (monitor line 1 um
     before the right PML). Returns a dict of AdjointFDTD2D arguments plus rho0 and the
-    material mapping."""
+    material mapping.
+
+    With ``wavelengths`` (a list), the source is a Gaussian-pulsed carrier at 1.55 um
+    (10 fs width, the signal of the dipole workload) and the objective has one term
+    per wavelength, each with the slab mode of that wavelength; ``rho_straight`` is
+    then the density of an uninterrupted guide (the transmission reference)."""
     from scipy.ndimage import gaussian_filter
 
     from .devices.mode import slab_mode_source
@@ -144,7 +149,10 @@ def topo_2d(n_designs=64, nx=600, ny=400, dx=0.02 * µm, n_steps=8000, pml=20, r
                    material=Material(12.25))
     t = np.arange(n_steps) * courant_dt(dx)
     f0 = LIGHT_SPEED / (1.55 * µm)
-    sig = ramped_cosine(t, amplitude=1.0, frequency=f0, phase=0, ramp_duration=20 / f0, t_max=t[-1] * 2)
+    if wavelengths is None:
+        sig = ramped_cosine(t, amplitude=1.0, frequency=f0, phase=0, ramp_duration=20 / f0, t_max=t[-1] * 2)
+    else:
+        sig = gaussian_pulse(t, 1.0, 3 * 10e-15, 10e-15, f0, 0.0)
     src = ModeSource(design=d, position=(pml * dx + 0.6 * µm, yc), width=2.0 * µm, wavelength=1.55 * µm, signal=sig,
                      direction="+x", num_modes=1)
     grid = RegularGrid(d, dx)
@@ -152,11 +160,31 @@ def topo_2d(n_designs=64, nx=600, ny=400, dx=0.02 * µm, n_steps=8000, pml=20, r
     mon = Monitor(start=(x_mon, yc - 1.0 * µm), end=(x_mon, yc + 1.0 * µm))
     pts = mon.get_grid_points_2d(dx, dx)
     ys = np.array([p[1] * dx for p in pts]) + 0.5 * dx - yc
-    mode, _ = slab_mode_source(x=ys, w=wg, n_WG=np.sqrt(12.25), n0=np.sqrt(2.085), wavelength=1.55 * µm, ind_m=0)
+    if wavelengths is None:
+        mode, _ = slab_mode_source(x=ys, w=wg, n_WG=np.sqrt(12.25), n0=np.sqrt(2.085), wavelength=1.55 * µm,
+                                   ind_m=0)
+        freq = f0
+    else:
+        mode = np.stack([slab_mode_source(x=ys, w=wg, n_WG=np.sqrt(12.25), n0=np.sqrt(2.085), wavelength=lam,
+                                          ind_m=0)[0] for lam in wavelengths])
+        freq = [LIGHT_SPEED / lam for lam in wavelengths]
     import torch
 
     rho = np.stack([gaussian_filter(torch.rand((r, r), generator=torch.Generator().manual_seed(seed + b),
                                                dtype=torch.float64).numpy(), sigma=3) for b in range(n_designs)])
+    straight = np.zeros((r, r))
+    rows = (np.arange(r) + y0 + 0.5) * dx
+    straight[(rows >= yc - wg / 2) & (rows <= yc + wg / 2), :] = 1.0
     return dict(eps_base=grid.permittivity, sigma=grid.conductivity, dx=dx, dt=t[1] - t[0], n_steps=n_steps,
-                sources=[src], monitor=mon, mode_profile=mode, frequency=f0, region=(y0, x0, r, r), rho0=rho,
-                eps_lo=2.085, eps_hi=12.25, design=d)
+                sources=[src], monitor=mon, mode_profile=mode, frequency=freq, region=(y0, x0, r, r), rho0=rho,
+                eps_lo=2.085, eps_hi=12.25, design=d, rho_straight=straight)
+
+
+SURROGATE_WAVELENGTHS = [1.50 * µm, 1.525 * µm, 1.55 * µm, 1.575 * µm, 1.60 * µm]
+
+
+def surrogate_2d(n_designs=64, seed=10000, n_steps=8000, **kw):
+    """The topology problem with a pulsed source and the transmission objective at
+    1.50, 1.525, 1.55, 1.575 and 1.60 um (the surrogate's outputs); densities from
+    seeds seed+b as in topo_2d."""
+    return topo_2d(n_designs=n_designs, seed=seed, n_steps=n_steps, wavelengths=SURROGATE_WAVELENGTHS, **kw)
