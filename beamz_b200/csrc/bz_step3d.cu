@@ -48,12 +48,12 @@ __device__ __forceinline__ void hfac(T a, const Geo3D<T>& g, T& fh, T& cx, T& cy
     cx = g.chx;
     cy = g.chy;
     cz = g.chz;
-  } else {
-    const T den = T(1) + a;
-    fh = (T(1) - a) / den;
-    cx = g.chx / den;
-    cy = g.chy / den;
-    cz = g.chz / den;
+  } else {  // (1-a)/(1+a) and c/(1+a) through one reciprocal
+    const T r = T(1) / (T(1) + a);
+    fh = (T(1) - a) * r;
+    cx = g.chx * r;
+    cy = g.chy * r;
+    cz = g.chz * r;
   }
 }
 
@@ -61,6 +61,14 @@ template <typename T>
 __device__ __forceinline__ T ld(const T* p, long long i, bool ok) {
   return ok ? __ldg(p + i) : T(0);
 }
+
+// Per-plane inputs of one thread's column: H, coefficients, and the E(x+1) / E(y+1)
+// values that the tile's last lane / last row read from memory.
+template <typename T, int NC>
+struct PlaneIn {
+  T hx[NC], hy[NC], hz[NC], ez_x[NC], ey_x[NC], ez_y[NC], ex_y[NC];
+  T a, ce;
+};
 
 template <typename T, int NC, int ZB>
 __global__ void __launch_bounds__(TX * TY) step3d_kernel(Ptr3<T> in, Out3<T> out, const T* __restrict__ ce,
@@ -75,6 +83,8 @@ __global__ void __launch_bounds__(TX * TY) step3d_kernel(Ptr3<T> in, Out3<T> out
   const int z1 = min(z0 + ZB, nz);
   const bool xin = x >= 0 && x < nx, yin = y >= 0 && y < ny, inb = xin && yin;
   const bool owned = inb && tx >= 1 && ty >= 1;
+  const bool xe = tx == TX - 1, ye = ty == TY - 1;
+  const bool xnb = yin && x + 1 < nx, ynb = xin && y + 1 < ny;
   const long long P = g.plane;
   const long long mb = (g.n_mat > 1 ? (long long)d : 0LL) * g.vol;
   const long long col = (long long)y * g.pitch + x;  // offset inside a plane
@@ -82,13 +92,36 @@ __global__ void __launch_bounds__(TX * TY) step3d_kernel(Ptr3<T> in, Out3<T> out
 #pragma unroll
   for (int c = 0; c < NC; ++c) fb[c] = ((long long)d * NC + c) * g.vol;
 
-  T exk[NC], eyk[NC], ezk[NC], hxm[NC], hym[NC];
+  // Loads of plane k's inputs; issued one plane ahead so they overlap the arithmetic.
+  auto load_plane = [&](int k, PlaneIn<T, NC>& q) {
+    const long long po = (long long)k * P + col;
+    q.a = ld(loss + mb, po, inb);
+    q.ce = ld(ce + mb, po, inb);
+#pragma unroll
+    for (int c = 0; c < NC; ++c) {
+      const long long o = fb[c] + po;
+      q.hx[c] = ld(in.h[0], o, inb);
+      q.hy[c] = ld(in.h[1], o, inb);
+      q.hz[c] = ld(in.h[2], o, inb);
+      q.ez_x[c] = ld(in.e[2], o + 1, xe && xnb);
+      q.ey_x[c] = ld(in.e[1], o + 1, xe && xnb);
+      q.ez_y[c] = ld(in.e[2], o + g.pitch, ye && ynb);
+      q.ex_y[c] = ld(in.e[0], o + g.pitch, ye && ynb);
+    }
+  };
+
+  T exk[NC], eyk[NC], ezk[NC], exn[NC], eyn[NC], ezn[NC], hxm[NC], hym[NC];
+  PlaneIn<T, NC> cur, nxt;
+  load_plane(z0, cur);
 #pragma unroll
   for (int c = 0; c < NC; ++c) {
     const long long o = fb[c] + (long long)z0 * P + col;
     exk[c] = ld(in.e[0], o, inb);
     eyk[c] = ld(in.e[1], o, inb);
     ezk[c] = ld(in.e[2], o, inb);
+    exn[c] = ld(in.e[0], o + P, inb && z0 + 1 < nz);
+    eyn[c] = ld(in.e[1], o + P, inb && z0 + 1 < nz);
+    ezn[c] = ld(in.e[2], o + P, inb && z0 + 1 < nz);
     hxm[c] = T(0);
     hym[c] = T(0);
   }
@@ -110,21 +143,24 @@ __global__ void __launch_bounds__(TX * TY) step3d_kernel(Ptr3<T> in, Out3<T> out
 
   for (int k = z0; k < z1; ++k) {
     const long long po = (long long)k * P + col;
-    const T a = ld(loss + mb, po, inb);
-    const T cev = ld(ce + mb, po, inb);
+    // prefetch: inputs of plane k+1 and E(k+2)
+    T ex2[NC], ey2[NC], ez2[NC];
+    if (k + 1 < z1) {
+      load_plane(k + 1, nxt);
+#pragma unroll
+      for (int c = 0; c < NC; ++c) {
+        const long long o = fb[c] + po + 2 * P;
+        ex2[c] = ld(in.e[0], o, inb && k + 2 < nz);
+        ey2[c] = ld(in.e[1], o, inb && k + 2 < nz);
+        ez2[c] = ld(in.e[2], o, inb && k + 2 < nz);
+      }
+    }
     T fh, cx, cy, cz;
-    hfac(a, g, fh, cx, cy, cz);
-    const T fe = T(1) - a * cev * g.inv_kd2;
-    T exn[NC], eyn[NC], ezn[NC], hx0[NC], hy0[NC], hz0[NC];
+    hfac(cur.a, g, fh, cx, cy, cz);
+    const T cev = cur.ce;
+    const T fe = T(1) - cur.a * cev * g.inv_kd2;
 #pragma unroll
     for (int c = 0; c < NC; ++c) {
-      const long long o = fb[c] + po;
-      exn[c] = ld(in.e[0], o + P, inb && k + 1 < nz);
-      eyn[c] = ld(in.e[1], o + P, inb && k + 1 < nz);
-      ezn[c] = ld(in.e[2], o + P, inb && k + 1 < nz);
-      hx0[c] = ld(in.h[0], o, inb);
-      hy0[c] = ld(in.h[1], o, inb);
-      hz0[c] = ld(in.h[2], o, inb);
       s_ez[c][ty][tx] = ezk[c];
       s_ex[c][ty][tx] = exk[c];
     }
@@ -132,24 +168,17 @@ __global__ void __launch_bounds__(TX * TY) step3d_kernel(Ptr3<T> in, Out3<T> out
     T hxn[NC], hyn[NC], hzn[NC];
 #pragma unroll
     for (int c = 0; c < NC; ++c) {
-      const long long o = fb[c] + po;
-      T ez_yp, ex_yp;
-      if (ty < TY - 1) {
-        ez_yp = s_ez[c][ty + 1][tx];
-        ex_yp = s_ex[c][ty + 1][tx];
-      } else {
-        ez_yp = ld(in.e[2], o + g.pitch, xin && y + 1 < ny && y >= -1);
-        ex_yp = ld(in.e[0], o + g.pitch, xin && y + 1 < ny && y >= -1);
-      }
+      const T ez_yp = ye ? cur.ez_y[c] : s_ez[c][ty + (ye ? 0 : 1)][tx];
+      const T ex_yp = ye ? cur.ex_y[c] : s_ex[c][ty + (ye ? 0 : 1)][tx];
       T ez_xp = __shfl_down_sync(FULL, ezk[c], 1);
       T ey_xp = __shfl_down_sync(FULL, eyk[c], 1);
-      if (tx == TX - 1) {
-        ez_xp = ld(in.e[2], o + 1, yin && x + 1 < nx);
-        ey_xp = ld(in.e[1], o + 1, yin && x + 1 < nx);
+      if (xe) {
+        ez_xp = cur.ez_x[c];
+        ey_xp = cur.ey_x[c];
       }
-      hxn[c] = fh * hx0[c] - (cy * (ez_yp - ezk[c]) - cz * (eyn[c] - eyk[c]));
-      hyn[c] = fh * hy0[c] - (cz * (exn[c] - exk[c]) - cx * (ez_xp - ezk[c]));
-      hzn[c] = fh * hz0[c] - (cx * (ey_xp - eyk[c]) - cy * (ex_yp - exk[c]));
+      hxn[c] = fh * cur.hx[c] - (cy * (ez_yp - ezk[c]) - cz * (eyn[c] - eyk[c]));
+      hyn[c] = fh * cur.hy[c] - (cz * (exn[c] - exk[c]) - cx * (ez_xp - ezk[c]));
+      hzn[c] = fh * cur.hz[c] - (cx * (ey_xp - eyk[c]) - cy * (ex_yp - exk[c]));
       s_hz[c][ty][tx] = hzn[c];
       s_hx[c][ty][tx] = hxn[c];
     }
@@ -180,9 +209,13 @@ __global__ void __launch_bounds__(TX * TY) step3d_kernel(Ptr3<T> in, Out3<T> out
       exk[c] = exn[c];
       eyk[c] = eyn[c];
       ezk[c] = ezn[c];
+      exn[c] = ex2[c];
+      eyn[c] = ey2[c];
+      ezn[c] = ez2[c];
       hxm[c] = hxn[c];
       hym[c] = hyn[c];
     }
+    cur = nxt;
   }
 }
 
