@@ -65,7 +65,7 @@ class Adjoint2D(C.Structure):
 
 class Gemm(C.Structure):
     _fields_ = [("M", i32), ("N", i32), ("K", i32), ("batch", i32), ("splitk", i32), ("act", i32), ("ta", i32),
-                ("tb", i32), ("atomic", i32), ("reserved", i32), ("A", vp), ("lda", i64), ("sa", i64), ("B", vp),
+                ("tb", i32), ("atomic", i32), ("engine", i32), ("A", vp), ("lda", i64), ("sa", i64), ("B", vp),
                 ("ldb", i64), ("sb", i64), ("alpha", C.c_float), ("reserved2", C.c_float), ("cadd", vp),
                 ("ldadd", i64), ("sadd", i64), ("bias_m", vp), ("bias_n", vp), ("outf", vp), ("outh", vp),
                 ("ldc", i64), ("sc", i64), ("pre", vp), ("ldpre", i64), ("spre", i64)]
@@ -145,12 +145,13 @@ _chan_sum = _sig("bz_chan_sum", C.c_int, [vp, vp, i32, i32, i32, vp])
 _adam = _sig("bz_adam", C.c_int, [vp, vp, vp, vp, vp, i64, C.c_float, C.c_float, C.c_float, C.c_float, i32,
                                   C.c_float, vp])
 _to_bf16 = _sig("bz_to_bf16", C.c_int, [vp, vp, i64, vp])
+_gemm_err = _sig("bz_gemm_error", C.c_int, [C.POINTER(i32), i32])
 
 #: every symbol include/beamz_b200.h declares (checked by the CPU test suite)
 EXPORTED = ["bz_version", "bz_last_error", "bz_step2d", "bz_step2d_multi", "bz_dft_fold", "bz_step2d_dft_static", "bz_advance_step",
             "bz_adjoint_step2d", "bz_step3d", "bz_cell_ops", "bz_gather", "bz_power3d", "bz_dft_fold_q", "bz_rasterize3d", "bz_prepare_coeffs", "bz_update_h2d",
             "bz_update_e2d", "bz_rasterize2d", "bz_gemm_bf16", "bz_spectral_mix", "bz_spectral_mix_bwd", "bz_gelu_bwd",
-            "bz_row_mean", "bz_row_broadcast", "bz_chan_sum", "bz_adam", "bz_to_bf16"]
+            "bz_row_mean", "bz_row_broadcast", "bz_chan_sum", "bz_adam", "bz_to_bf16", "bz_gemm_error"]
 
 
 class NativeError(RuntimeError):
@@ -272,3 +273,10 @@ def adam(w, g, m, v, wh, n, lr, b1, b2, eps, step, wd, stream) -> None:
 
 def to_bf16(x, y, n, stream) -> None:
     check(_to_bf16(x, y, n, stream))
+
+
+def gemm_error(reset: bool = True) -> int:
+    """Error word of the tcgen05 GEMM (non-zero: a bounded pipeline wait ran out)."""
+    v = i32(0)
+    check(_gemm_err(C.byref(v), 1 if reset else 0))
+    return v.value

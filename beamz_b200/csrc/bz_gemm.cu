@@ -231,6 +231,216 @@ int launch_gemm(const GemmP& p, cudaStream_t st) {
   return check_launch("bz_gemm_bf16");
 }
 
+
+// ---- tcgen05 path: A row-major (K contiguous) x B stored [N][K] (K contiguous) ------
+// One CTA of 128 threads computes a 128 x 256 tile into 256 TMEM columns (f32). Per
+// 64-wide K slice, the threads stage A (128 x 64) and B (256 x 64) in shared memory in
+// the no-swizzle K-major core-matrix layout (8 rows x 16 bytes per core matrix; 8-row
+// groups 128 bytes apart, K chunks LBO apart, LBO padded by 16 bytes so that the
+// 16-byte stores of a warp spread over all banks); one thread issues four
+// tcgen05.mma (K = 16 each, kind::f16 with bf16 A and B) and commits them to the
+// stage's mbarrier. Two stages: the next slice's global loads overlap the MMAs. The
+// epilogue reads the accumulators with tcgen05.ld (warp w owns rows 32w..32w+31).
+// Every mbarrier wait is bounded; a timeout raises g_tc_error and the CTA frees its
+// TMEM and returns.
+namespace tc {
+constexpr int BM = 128, BN = 256, BK = 64, THREADS = 128;
+constexpr int LBO_A = (BM / 8) * 128 + 16, LBO_B = (BN / 8) * 128 + 16;
+constexpr int A_BYTES = 8 * LBO_A, B_BYTES = 8 * LBO_B;  // 8 K chunks of 8 elements
+constexpr int STAGE = A_BYTES + B_BYTES;
+constexpr int SMEM = 2 * STAGE + 64;
+constexpr uint32_t IDESC = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BN >> 3) << 17) |
+                           ((uint32_t)(BM >> 4) << 24);  // f32 accum, bf16 A/B, K-major, M=128, N=256
+constexpr int WAIT_LIMIT = 1 << 22;
+}  // namespace tc
+
+__device__ int g_tc_error = 0;
+
+__device__ __forceinline__ uint64_t tc_sdesc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+  uint64_t d = (uint64_t)((saddr >> 4) & 0x3FFFu);
+  d |= (uint64_t)((lbo >> 4) & 0x3FFFu) << 16;
+  d |= (uint64_t)((sbo >> 4) & 0x3FFFu) << 32;
+  d |= (uint64_t)1 << 46;  // descriptor version of sm_100; base offset 0, no swizzle
+  return d;
+}
+
+__device__ __forceinline__ bool tc_wait(uint32_t mbar, uint32_t parity) {
+  for (int i = 0; i < tc::WAIT_LIMIT; ++i) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(ok)
+        : "r"(mbar), "r"(parity)
+        : "memory");
+    if (ok) return true;
+  }
+  return false;
+}
+
+__global__ void __launch_bounds__(tc::THREADS) gemm_tc_kernel(GemmP p) {
+  extern __shared__ __align__(128) unsigned char smem[];
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int bz = blockIdx.z / p.splitk, ks = blockIdx.z % p.splitk;
+  const int m0 = blockIdx.y * tc::BM, n0 = blockIdx.x * tc::BN;
+  const bf16* A = p.A + (long long)bz * p.sa;
+  const bf16* B = p.B + (long long)bz * p.sb;
+  const int ktiles = (p.K + tc::BK - 1) / tc::BK;
+  const int kper = (ktiles + p.splitk - 1) / p.splitk;
+  const int kt0 = ks * kper, kt1 = min(ktiles, kt0 + kper);
+  uint64_t* mbar = reinterpret_cast<uint64_t*>(smem + 2 * tc::STAGE);
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(smem + 2 * tc::STAGE + 16);
+  const uint32_t sbase = static_cast<uint32_t>(__cvta_generic_to_shared(smem));
+  const uint32_t mb0 = static_cast<uint32_t>(__cvta_generic_to_shared(&mbar[0]));
+
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(
+                     static_cast<uint32_t>(__cvta_generic_to_shared(tmem_slot))),
+                 "r"(tc::BN));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::);
+  }
+  if (tid == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(mb0));
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(mb0 + 8));
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;\n" ::);
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
+  const uint32_t taddr = *tmem_slot;
+
+  // global -> registers: A 8 chunks and B 16 chunks of 16 bytes per thread
+  uint4 ra[8], rb[16];
+  auto gload = [&](int kt) {
+    const int k0 = kt * tc::BK;
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+      const int c = tid + i * tc::THREADS, r = c >> 3, j = c & 7;
+      const int m = m0 + r;
+      ra[i] = load8(A + (long long)min(m, p.M - 1) * p.lda, k0 + j * 8, p.K, m < p.M);
+    }
+#pragma unroll
+    for (int i = 0; i < 16; ++i) {
+      const int c = tid + i * tc::THREADS, r = c >> 3, j = c & 7;
+      const int n = n0 + r;
+      rb[i] = load8(B + (long long)min(n, p.N - 1) * p.ldb, k0 + j * 8, p.K, n < p.N);
+    }
+  };
+  auto sstore = [&](int s) {
+    unsigned char* st = smem + s * tc::STAGE;
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+      const int c = tid + i * tc::THREADS, r = c >> 3, j = c & 7;
+      *reinterpret_cast<uint4*>(st + j * tc::LBO_A + (r >> 3) * 128 + (r & 7) * 16) = ra[i];
+    }
+#pragma unroll
+    for (int i = 0; i < 16; ++i) {
+      const int c = tid + i * tc::THREADS, r = c >> 3, j = c & 7;
+      *reinterpret_cast<uint4*>(st + tc::A_BYTES + j * tc::LBO_B + (r >> 3) * 128 + (r & 7) * 16) = rb[i];
+    }
+  };
+
+  uint32_t phase[2] = {0u, 0u};
+  bool ok = true;
+  int last = -1;
+  if (kt0 < kt1) {
+    gload(kt0);
+    sstore(0);
+    for (int kt = kt0; kt < kt1 && ok; ++kt) {
+      const int s = (kt - kt0) & 1;
+      asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+      __syncthreads();
+      if (tid == 0) {
+        asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
+        const uint32_t a0 = sbase + s * tc::STAGE, b0 = a0 + tc::A_BYTES;
+#pragma unroll
+        for (int kk = 0; kk < tc::BK / 16; ++kk) {
+          const uint64_t da = tc_sdesc(a0 + kk * 2 * tc::LBO_A, tc::LBO_A, 128);
+          const uint64_t db = tc_sdesc(b0 + kk * 2 * tc::LBO_B, tc::LBO_B, 128);
+          const uint32_t acc = (kt > kt0 || kk > 0) ? 1u : 0u;
+          asm volatile(
+              "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+              "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n"
+              :
+              : "r"(taddr), "l"(da), "l"(db), "r"(tc::IDESC), "r"(acc), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
+        }
+        asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(
+            mb0 + 8 * s));
+      }
+      last = s;
+      if (kt + 1 < kt1) {
+        gload(kt + 1);
+        const int s2 = s ^ 1;
+        if (kt > kt0) {  // the MMAs of the previous slice read stage s2
+          ok = tc_wait(mb0 + 8 * s2, phase[s2]);
+          phase[s2] ^= 1u;
+        }
+        if (ok) sstore(s2);
+      }
+      ok = __syncthreads_and(ok);
+    }
+    if (ok) {
+      ok = tc_wait(mb0 + 8 * last, phase[last]);
+    } else {
+      tc_wait(mb0 + 8 * last, phase[last]);  // let issued MMAs drain before the TMEM goes
+    }
+    if (!ok && tid == 0) atomicExch(&g_tc_error, 1);
+  }
+  asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
+  // epilogue: thread (warp w, lane l) owns row 32w + l of the tile
+  const int m = m0 + warp * 32 + lane;
+  if (__syncthreads_and(ok)) {
+    for (int c0 = 0; c0 < tc::BN; c0 += 8) {
+      uint32_t v[8];
+      if (kt0 < kt1) {
+        asm volatile(
+            "tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];\n"
+            : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7])
+            : "r"(taddr + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0));
+        asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+      } else {
+#pragma unroll
+        for (int e = 0; e < 8; ++e) v[e] = 0u;
+      }
+#pragma unroll
+      for (int e = 0; e < 8; ++e) {
+        const int n = n0 + c0 + e;
+        if (m >= p.M || n >= p.N) continue;
+        float x = p.alpha * __uint_as_float(v[e]);
+        if (p.cadd) x += p.cadd[(long long)bz * p.sadd + (long long)m * p.ldadd + n];
+        if (p.bias_m) x += p.bias_m[m];
+        if (p.bias_n) x += p.bias_n[n];
+        if (p.pre) p.pre[(long long)bz * p.spre + (long long)m * p.ldpre + n] = __float2bfloat16_rn(x);
+        if (p.act == 1) x = gelu_f(x);
+        const long long o = (long long)bz * p.sc + (long long)m * p.ldc + n;
+        if (p.outf) {
+          if (p.atomic) atomicAdd(p.outf + o, x); else p.outf[o] = x;
+        }
+        if (p.outh) p.outh[o] = __float2bfloat16_rn(x);
+      }
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;\n" ::);
+  __syncthreads();
+  if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(taddr), "r"(tc::BN));
+}
+
+int launch_gemm_tc(const GemmP& p, cudaStream_t st) {
+  static bool configured = false;
+  if (!configured) {
+    if (cudaFuncSetAttribute(gemm_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, tc::SMEM) != cudaSuccess)
+      return fail(BZ_ERR_CUDA, "bz_gemm_bf16: cannot configure the tcgen05 kernel's shared memory");
+    configured = true;
+  }
+  dim3 grid((unsigned)ceil_div(p.N, tc::BN), (unsigned)ceil_div(p.M, tc::BM), (unsigned)(p.batch * p.splitk));
+  gemm_tc_kernel<<<grid, tc::THREADS, tc::SMEM, st>>>(p);
+  return check_launch("bz_gemm_bf16");
+}
+
+bool tc_eligible(const GemmP& p) {
+  auto al = [](const void* q) { return (reinterpret_cast<uintptr_t>(q) & 15u) == 0u; };
+  return !p.ta && p.tb && p.M >= 128 && p.N >= 256 && p.K >= 64 && p.lda % 8 == 0 && p.ldb % 8 == 0 &&
+         p.sa % 8 == 0 && p.sb % 8 == 0 && al(p.A) && al(p.B);
+}
+
 // ---- spectral channel mixing: O[b][o][k] = sum_c U[b][c][k] * W[k][c][o] (complex) ---
 // U, O: [B][C][n_modes][2] bf16 (re, im); W: [n_modes][Ci][Co][2] bf16.
 __global__ void spectral_fwd_kernel(const bf16* __restrict__ U, const bf16* __restrict__ W, bf16* __restrict__ O,
@@ -391,9 +601,24 @@ extern "C" int bz_gemm_bf16(const bz_gemm* g, void* stream) {
   p.outf = g->outf; p.outh = (bz::bf16*)g->outh; p.ldc = g->ldc; p.sc = g->sc;
   p.pre = (bz::bf16*)g->pre; p.ldpre = g->ldpre; p.spre = g->spre;
   cudaStream_t st = bz::as_stream(stream);
+  if (g->engine == 0 && bz::tc_eligible(p)) return bz::launch_gemm_tc(p, st);
   if (g->N <= 32) return bz::launch_gemm<128, 32, 4, 1>(p, st);
   if (g->M <= 32) return bz::launch_gemm<32, 128, 1, 4>(p, st);
   return bz::launch_gemm<128, 128, 2, 4>(p, st);
+}
+
+extern "C" int bz_gemm_error(int32_t* value, int32_t reset) {
+  BZ_REQUIRE(value != nullptr, "bz_gemm_error: NULL value");
+  int v = 0;
+  if (cudaMemcpyFromSymbol(&v, bz::g_tc_error, sizeof(int)) != cudaSuccess)
+    return bz::fail(BZ_ERR_CUDA, "bz_gemm_error: cannot read the error word");
+  *value = v;
+  if (reset && v) {
+    const int zero = 0;
+    if (cudaMemcpyToSymbol(bz::g_tc_error, &zero, sizeof(int)) != cudaSuccess)
+      return bz::fail(BZ_ERR_CUDA, "bz_gemm_error: cannot reset the error word");
+  }
+  return BZ_OK;
 }
 
 extern "C" int bz_spectral_mix(const void* U, const void* W, void* O, int32_t B, int32_t ci, int32_t co,

@@ -98,7 +98,7 @@ class AdjointFDTD2D:
             full, er = self._eps_full(eps_region)
             self.engine = Engine2D(full, self.sigma, self.dx, self.dx, self.dt, self.n_steps, self.sources,
                                    [self.monitor], precision=self.precision, n_comp=1, n_designs=self.B,
-                                   record=False, use_graphs=True)
+                                   record=False, use_graphs=True, time_block="auto")
             dev = self.engine.dev
             self._eps_t = torch.as_tensor(self.eps_base).to(dev)
             self._sigma_t = torch.as_tensor(self.sigma).to(dev).expand(self.B, self.ny, self.nx).contiguous()

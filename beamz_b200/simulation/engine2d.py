@@ -20,6 +20,9 @@ from .compile_ops import SourceOps, compile_monitors_2d, compile_sources
 
 GRAPH_CHUNK = 64  # at most this many steps per captured graph
 RING_LEN = GRAPH_CHUNK  # monitor samples kept between DFT folds
+# (steps per launch, register-tile shape) tried by the autotuner
+TUNE_CANDIDATES = ((7, 0), (7, 1), (7, 3), (5, 0), (5, 1), (3, 1))
+_TUNED: dict = {}  # (device name, nx, ny, designs, components, dtype) -> (time_block, tb_tile)
 
 
 def _round_up(n: int, m: int) -> int:
@@ -68,10 +71,14 @@ class Engine2D:
         self.d_step = torch.zeros(1, dtype=torch.int64, device=self.dev)
         self.use_graphs = use_graphs
         self._graphs: dict[int, torch.cuda.CUDAGraph] = {}
+        self._autotune = time_block == "auto"
+        if self._autotune:
+            time_block = 7
         if int(time_block) not in (1, 3, 5, 7):
-            raise ValueError(f"time_block must be 1, 3, 5 or 7 (got {time_block})")
+            raise ValueError(f"time_block must be 1, 3, 5, 7 or 'auto' (got {time_block})")
         # power accumulation runs on the single-step kernel
         self.time_block = 1 if power else int(time_block)
+        self._autotune = self._autotune and not power
         self.tb_tile = int(tb_tile)
         self.chunk = GRAPH_CHUNK // self.time_block * self.time_block  # steps per graph
         self.n_step_launches = 0  # step-kernel launches issued (graph nodes included)
@@ -259,8 +266,38 @@ class Engine2D:
             self._graphs[phase] = g
         return g
 
+    def autotune(self, candidates=TUNE_CANDIDATES, launches: int = 4):
+        """Pick (time_block, tb_tile) by timing blocked launches on this grid (CUDA events).
+
+        Every candidate gives the same results (same arithmetic per cell), and a launch
+        only writes the copy that the next step overwrites and ring/record slots of steps
+        not yet taken, so timing from the current state changes nothing. The choice is
+        cached per (device, grid, designs, components, dtype) for the process."""
+        key = (torch.cuda.get_device_name(self.dev), self.nx, self.ny, self.n_designs, self.n_comp, self.bz_dtype)
+        if key not in _TUNED:
+            times = {}
+            for tb, tile in candidates:
+                self.time_block, self.tb_tile = tb, tile
+                self._launch_tb(self.step_index, None)  # warm-up
+                a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                a.record()
+                for _ in range(launches):
+                    self._launch_tb(self.step_index, None)
+                b.record()
+                b.synchronize()
+                times[(tb, tile)] = a.elapsed_time(b) / (launches * tb)
+            _TUNED[key] = min(times, key=times.get)
+            self.tune_times = times
+        self.time_block, self.tb_tile = _TUNED[key]
+        self.chunk = GRAPH_CHUNK // self.time_block * self.time_block
+        self._graphs.clear()
+        self._autotune = False
+        return _TUNED[key]
+
     def run_steps(self, n: int):
         """Advance n steps, replaying graph chunks where the record buffer allows."""
+        if self._autotune:
+            self.autotune()
         while n > 0:
             self._maybe_drain()
             room = n

@@ -119,7 +119,7 @@ class FDTD:
             self.engine = Engine2D(self.mesh.permittivity, self.mesh.conductivity, self.dx, self.dy, self.dt,
                                    self.num_steps, self.sources, self.monitors, precision=precision, n_comp=n_comp,
                                    power=accumulate_power, use_graphs=graphs, tile_rows=opts.get("tile_rows", 16),
-                                   time_block=opts.get("time_block", 7), tb_tile=opts.get("tb_tile", 0))
+                                   time_block=opts.get("time_block", "auto"), tb_tile=opts.get("tb_tile", 0))
 
     def __getattr__(self, name):
         # field access with the reference's names and shapes (device tensors)

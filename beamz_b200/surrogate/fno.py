@@ -67,6 +67,9 @@ class FNO2d:
         F, G = spectral_bases(n, modes)
         self.F = torch.as_tensor(F, dtype=torch.float32).to(self.dev).to(BF16)
         self.G = torch.as_tensor(G, dtype=torch.float32).to(self.dev).to(BF16)
+        # transposed copies: every large GEMM then reads its B operand K-contiguous
+        self.FT = self.F.t().contiguous()  # [2K][P]
+        self.GT = self.G.t().contiguous()  # [P][2K]
         gen = torch.Generator().manual_seed(seed)
         C, Hd = width, head
 
@@ -85,6 +88,9 @@ class FNO2d:
         self.params["q1"] = _Param(rnd(Hd, scale=0.0))
         self.params["Q2"] = _Param(rnd(n_out, Hd, scale=1 / math.sqrt(Hd)))
         self.params["q2"] = _Param(rnd(n_out, scale=0.0))
+        # outputs are y = raw * y_scale + y_shift (targets standardised for training)
+        self.y_scale = torch.ones(n_out, device=self.dev)
+        self.y_shift = torch.zeros(n_out, device=self.dev)
         self.step_count = 0
         self._acts = None
         self.flops = 0.0  # tensor-core FLOPs issued (2*M*N*K per GEMM), for throughput reports
@@ -110,12 +116,16 @@ class FNO2d:
         nat.gemm(g, self._stream())
         self.flops += 2.0 * M * N * K * batch
 
+    @staticmethod
+    def _split(M, N):
+        """K splits giving about two CTAs of 128 x 256 output tiles per SM."""
+        return max(1, min(16, 296 // max(1, ((M + 127) // 128) * ((N + 255) // 256))))
+
     def _dft(self, V, B):
         """U = V [B*C x P] @ F [P x 2K] (split over P, f32 atomics) -> bf16."""
         BC, K2 = B * self.C, 2 * self.K
         acc = torch.zeros((BC, K2), dtype=torch.float32, device=self.dev)
-        split = max(1, min(8, 148 * 2 // max(1, ((BC + 127) // 128) * ((K2 + 127) // 128))))
-        self._gemm(BC, K2, self.P, V, self.P, self.F, K2, outf=acc, atomic=1, splitk=split)
+        self._gemm(BC, K2, self.P, V, self.P, self.FT, self.P, tb=1, outf=acc, atomic=1, splitk=self._split(BC, K2))
         out = torch.empty((BC, K2), dtype=BF16, device=self.dev)
         nat.to_bf16(acc.data_ptr(), out.data_ptr(), acc.numel(), self._stream())
         return out
@@ -124,8 +134,7 @@ class FNO2d:
         """D [B*C x P] @ G^T -> bf16 [B*C x 2K] (gradient through the inverse transform)."""
         BC, K2 = B * self.C, 2 * self.K
         acc = torch.zeros((BC, K2), dtype=torch.float32, device=self.dev)
-        split = max(1, min(8, 148 * 2 // max(1, ((BC + 127) // 128) * ((K2 + 127) // 128))))
-        self._gemm(BC, K2, self.P, D, self.P, self.G, self.P, tb=1, outf=acc, atomic=1, splitk=split)
+        self._gemm(BC, K2, self.P, D, self.P, self.G, self.P, tb=1, outf=acc, atomic=1, splitk=self._split(BC, K2))
         out = torch.empty((BC, K2), dtype=BF16, device=self.dev)
         nat.to_bf16(acc.data_ptr(), out.data_ptr(), acc.numel(), self._stream())
         return out
@@ -153,7 +162,7 @@ class FNO2d:
             O = torch.empty_like(U)
             nat.spectral_mix(U.data_ptr(), p[f"R{l}"].h.data_ptr(), O.data_ptr(), B, C, C, self.K, self._stream())
             S = torch.empty((B * C, P), dtype=torch.float32, device=self.dev)
-            self._gemm(B * C, P, 2 * self.K, O, 2 * self.K, self.G, P, outf=S)
+            self._gemm(B * C, P, 2 * self.K, O, 2 * self.K, self.GT, 2 * self.K, tb=1, outf=S)
             act = 1 if l < self.L else 0
             pre = torch.empty((B, C, P), dtype=BF16, device=self.dev) if act else None
             Vn = torch.empty((B, C, P), dtype=BF16, device=self.dev)
@@ -173,6 +182,7 @@ class FNO2d:
         pooled_h = pooled.to(BF16)
         out = torch.empty((B, self.n_out), dtype=torch.float32, device=self.dev)
         self._gemm(B, self.n_out, Hd, pooled_h, Hd, p["Q2"].h, Hd, tb=1, outf=out, bias_n=p["q2"].w)
+        out = out * self.y_scale[None, :] + self.y_shift[None, :]
         if keep:
             acts.update(preh=preh, pooled_h=pooled_h, B=B)
             self._acts = acts
@@ -190,7 +200,7 @@ class FNO2d:
         p, C, P, Hd, B = self.params, self.C, self.P, self.Hd, a["B"]
         st = self._stream()
         split = lambda k: max(1, min(16, k // 2048))  # noqa: E731
-        dO = d_out.float().contiguous()
+        dO = (d_out.float() * self.y_scale[None, :]).contiguous()
         dOh = dO.to(BF16)
         p["q2"].g += dO.sum(0)
         self._gemm(self.n_out, Hd, B, dOh, self.n_out, a["pooled_h"], Hd, ta=1, outf=p["Q2"].g, atomic=1)
@@ -245,10 +255,17 @@ class FNO2d:
                      b1, b2, eps, self.step_count, weight_decay, self._stream())
 
     def state_dict(self) -> dict:
-        return {k: q.w.detach().cpu() for k, q in self.params.items()}
+        sd = {k: q.w.detach().cpu().clone() for k, q in self.params.items()}
+        sd["_y_scale"], sd["_y_shift"] = self.y_scale.cpu().clone(), self.y_shift.cpu().clone()
+        return sd
 
     def load_state_dict(self, sd: dict):
         for k, v in sd.items():
-            q = self.params[k]
-            q.w.copy_(v.to(q.w.device))
-            q.h.copy_(q.w.to(BF16))
+            if k == "_y_scale":
+                self.y_scale.copy_(v.to(self.dev))
+            elif k == "_y_shift":
+                self.y_shift.copy_(v.to(self.dev))
+            else:
+                q = self.params[k]
+                q.w.copy_(v.to(q.w.device))
+                q.h.copy_(q.w.to(BF16))

@@ -7,14 +7,16 @@ mode transmission T_f = |a_f|^2 / |a_f(straight guide)|^2 at the output monitor.
 * ``TransmissionProblem`` evaluates T for a batch of densities with one batched FDTD
   forward (``AdjointFDTD2D``), and the exact gradient of the mean transmission with
   the batched adjoint.
-* ``make_dataset`` draws smoothed random densities and labels them with batched FDTD.
+* ``make_dataset`` draws smoothed random densities (optionally also the designs visited
+  by batched exact-adjoint ascents from random starts) and labels them with batched FDTD.
 * ``train`` fits the FNO surrogate (bf16 kernels, f32 accumulation) on them.
 * ``SurrogateSearch`` runs the loop: the surrogate proposes candidates around the
   current design (steps along its own input gradient plus smooth perturbations), the
   best-ranked are verified by one batched FDTD forward, and the best verified one is
   kept if it improves; whenever the surrogate misses the verified transmission by more
-  than ``tol`` (or proposes nothing better), that round takes a plain exact-adjoint
-  step instead and the verified samples are added to the surrogate's training set.
+  than ``tol`` (or proposes nothing better), that round also takes a plain exact-adjoint
+  step (verified together with the next round's candidates) and fine-tunes the
+  surrogate on the verified samples.
 * ``plain_adjoint`` is the baseline: the same ascent with the exact adjoint gradient,
   one design per FDTD call.
 """
@@ -101,8 +103,9 @@ class TransmissionProblem:
         self.fdtd_designs += len(rho)
         return out
 
-    def value_and_grad(self, rho):
-        """Mean transmission (B,) and its exact gradient with respect to rho (B, r, r)."""
+    def value_and_grad(self, rho, return_T=False):
+        """Mean transmission (B,) and its exact gradient with respect to rho (B, r, r)
+        (and T (B, n_freq) when asked)."""
         rho = np.asarray(rho)
         t0 = time.perf_counter()
         p = self._problem(len(rho))
@@ -110,44 +113,74 @@ class TransmissionProblem:
         torch.cuda.synchronize()
         self.fdtd_seconds += time.perf_counter() - t0
         self.fdtd_designs += len(rho)
-        return J, g * (self.eps_hi - self.eps_lo)
+        g = g * (self.eps_hi - self.eps_lo)
+        if return_T:
+            return J, g, p.power / self.ref_power[None, :]
+        return J, g
 
 
-def make_dataset(problem: TransmissionProblem, n_samples: int, seed0: int = 10000, batch: int = 64):
-    """(rho (n, r, r) float32, T (n, n_freq) float32) labelled by batched FDTD."""
+def make_dataset(problem: TransmissionProblem, n_samples: int, seed0: int = 10000, batch: int = 64,
+                 trajectory_frac: float = 0.0, step: float = 0.05):
+    """(rho (n, r, r) float32, T (n, n_freq) float32) labelled by batched FDTD.
+
+    A fraction ``trajectory_frac`` comes from exact-adjoint ascent trajectories (``batch``
+    random starts stepped together with the batched adjoint, every visited design kept),
+    so that the set also covers the high-transmission designs an optimiser reaches; the
+    rest are independent smoothed random densities."""
     r = problem.kw["region"][2]
-    rho = densities(range(seed0, seed0 + n_samples), r)
+    n_traj = int(round(n_samples * trajectory_frac)) // batch * batch
+    n_rand = n_samples - n_traj
+    rho = np.empty((n_samples, r, r), dtype=np.float32)
     T = np.empty((n_samples, problem.n_freq), dtype=np.float32)
-    for i in range(0, n_samples, batch):
+    rho[:n_rand] = densities(range(seed0, seed0 + n_rand), r)
+    for i in range(0, n_rand, batch):
         T[i:i + batch] = problem.transmission(rho[i:i + batch])
+    cur = torch.as_tensor(densities(range(seed0 + n_rand, seed0 + n_rand + batch), r), dtype=torch.float64)
+    for i in range(n_rand, n_samples, batch):
+        _, g, Tb = problem.value_and_grad(cur.numpy(), return_T=True)
+        rho[i:i + batch], T[i:i + batch] = cur.numpy(), Tb
+        cur = _ascend(cur, torch.as_tensor(g), step)
     return rho, T
 
 
 def train(net: FNO2d, rho: np.ndarray, T: np.ndarray, epochs: int = 20, batch: int = 64, lr: float = 2e-3,
-          seed: int = 0, log=None) -> list[float]:
-    """MSE fit of T with Adam and a cosine learning-rate decay; returns per-epoch losses."""
+          seed: int = 0, val_frac: float = 0.05, weight_decay: float = 1e-4, log=None) -> dict:
+    """MSE fit of T (targets standardised per output) with Adam, a cosine learning-rate
+    decay and weight decay; a held-out split picks the best epoch, whose weights are kept.
+    Returns {"train": per-epoch MSE, "val": per-epoch validation MAE, "best_epoch"}."""
     rng = np.random.default_rng(seed)
-    n = len(rho)
+    order = rng.permutation(len(rho))
+    n_val = max(1, int(len(rho) * val_frac))
+    val, tr = order[:n_val], order[n_val:]
+    n = len(tr)
     rho_d = torch.as_tensor(rho, device=net.dev)
     T_d = torch.as_tensor(T, device=net.dev)
+    net.y_shift.copy_(T_d[tr].mean(0))
+    net.y_scale.copy_(T_d[tr].std(0).clamp_min(1e-6))
     steps = epochs * ((n + batch - 1) // batch)
-    k, losses = 0, []
+    k, losses, vals, best = 0, [], [], (np.inf, -1, None)
     for ep in range(epochs):
-        perm = torch.as_tensor(rng.permutation(n), device=net.dev)
+        perm = torch.as_tensor(tr[rng.permutation(n)], device=net.dev)
         tot = 0.0
         for i in range(0, n, batch):
             idx = perm[i:i + batch]
             out = net.forward(rho_d[idx], keep=True)
-            err = out - T_d[idx]
+            err = (out - T_d[idx]) / net.y_scale[None, :]
             tot += float((err ** 2).sum())
             net.zero_grad()
-            net.backward(2.0 * err / err.numel())
-            net.adam_step(lr=lr * 0.5 * (1 + np.cos(np.pi * k / steps)))
+            net.backward(2.0 * err / (err.numel() * net.y_scale[None, :]))
+            net.adam_step(lr=lr * 0.5 * (1 + np.cos(np.pi * k / steps)), weight_decay=weight_decay)
             k += 1
         losses.append(tot / (n * T.shape[1]))
+        vi = torch.as_tensor(val, device=net.dev)
+        pred = torch.cat([net.forward(rho_d[vi[i:i + 256]]) for i in range(0, n_val, 256)])
+        vals.append(float((pred - T_d[vi]).abs().mean()))
+        if vals[-1] < best[0]:
+            best = (vals[-1], ep, net.state_dict())
         if log:
-            log(f"epoch {ep}: mse {losses[-1]:.3e}")
-    return losses
+            log(f"epoch {ep}: standardised mse {losses[-1]:.3e}, validation mae {vals[-1]:.4f}")
+    net.load_state_dict(best[2])
+    return {"train": losses, "val": vals, "best_epoch": best[1]}
 
 
 def _ascend(rho: torch.Tensor, g: torch.Tensor, step) -> torch.Tensor:
@@ -172,12 +205,13 @@ def plain_adjoint(problem: TransmissionProblem, rho0: np.ndarray, iterations: in
 
 class SurrogateSearch:
     def __init__(self, problem: TransmissionProblem, net: FNO2d, n_candidates=256, n_verify=16, tol=1e-2,
-                 adjoint_step=0.05, seed=0):
+                 adjoint_step=0.05, seed=0, replay=None):
         self.problem, self.net = problem, net
         self.n_cand, self.n_verify, self.tol = n_candidates, n_verify, tol
         self.adjoint_step = adjoint_step
         self.gen = torch.Generator(device=net.dev).manual_seed(seed)
         self.rho_new, self.T_new = [], []  # verified samples collected for fine-tuning
+        self.replay = replay  # (rho, T) of the training set, mixed into fine-tuning batches
         self.log = []
 
     def _predict(self, rho: torch.Tensor) -> torch.Tensor:
@@ -200,17 +234,24 @@ class SurrogateSearch:
         cand = rho[None] + steps.double()[:, None, None] * gg + amp.double() * noise.double()
         return smooth(cand, 1).clamp(0.0, 1.0)
 
-    def _finetune(self, steps=20, lr=5e-4):
+    def _finetune(self, steps=10, lr=5e-4):
         if not self.rho_new:
             return
-        rho = torch.as_tensor(np.concatenate(self.rho_new), dtype=torch.float32, device=self.net.dev)
-        T = torch.as_tensor(np.concatenate(self.T_new), dtype=torch.float32, device=self.net.dev)
+        dev = self.net.dev
+        rho = torch.as_tensor(np.concatenate(self.rho_new), dtype=torch.float32, device=dev)
+        T = torch.as_tensor(np.concatenate(self.T_new), dtype=torch.float32, device=dev)
+        rng = np.random.default_rng(len(self.rho_new))
         for _ in range(steps):
-            idx = torch.randint(0, len(rho), (min(64, len(rho)),), generator=self.gen, device=self.net.dev)
-            out = self.net.forward(rho[idx], keep=True)
-            err = out - T[idx]
+            idx = torch.randint(0, len(rho), (min(32, len(rho)),), generator=self.gen, device=dev)
+            xb, yb = rho[idx], T[idx]
+            if self.replay is not None:  # half of each batch from the training set
+                j = rng.integers(0, len(self.replay[0]), 32)
+                xb = torch.cat([xb, torch.as_tensor(self.replay[0][j], device=dev)])
+                yb = torch.cat([yb, torch.as_tensor(self.replay[1][j], device=dev)])
+            out = self.net.forward(xb, keep=True)
+            err = (out - yb) / self.net.y_scale[None, :]
             self.net.zero_grad()
-            self.net.backward(2.0 * err / err.numel())
+            self.net.backward(2.0 * err / (err.numel() * self.net.y_scale[None, :]))
             self.net.adam_step(lr=lr)
 
     def run(self, rho0: np.ndarray, rounds: int, target: float | None = None):
@@ -221,27 +262,27 @@ class SurrogateSearch:
         best = float(self.problem.transmission(rho[None].cpu().numpy()).mean())
         hist = [best]
         t0 = time.perf_counter()
+        pending = None  # exact-adjoint step awaiting verification with the next candidates
         for rnd in range(rounds):
             cand = self._proposals(rho)
             pred = self._predict(cand).mean(dim=1)
             top = torch.topk(pred, self.n_verify).indices
             chosen = cand[top]
-            T_true = self.problem.transmission(chosen.cpu().numpy())
+            batch = chosen if pending is None else torch.cat([chosen, pending.to(dev)[None]])
+            T_true = self.problem.transmission(batch.cpu().numpy())
             t_true = T_true.mean(axis=1)
-            err = float(np.abs(pred[top].double().cpu().numpy() - t_true).max())
+            err = float(np.abs(pred[top].double().cpu().numpy() - t_true[:self.n_verify]).max())
             self.rho_new.append(chosen.float().cpu().numpy())
-            self.T_new.append(T_true.astype(np.float32))
+            self.T_new.append(T_true[:self.n_verify].astype(np.float32))
             k = int(np.argmax(t_true))
-            improved = t_true[k] > best
-            if improved:
-                best, rho = float(t_true[k]), chosen[k]
-            fallback = err > self.tol or not improved
+            surrogate_gain = t_true[:self.n_verify].max() > best
+            if t_true[k] > best:
+                best, rho = float(t_true[k]), batch[k]
+            fallback = err > self.tol or not surrogate_gain
+            pending = None
             if fallback:
-                J, g = self.problem.value_and_grad(rho[None].cpu().numpy())
-                nxt = _ascend(rho[None].cpu(), torch.as_tensor(g), self.adjoint_step)
-                t_next = float(self.problem.transmission(nxt.numpy()).mean())
-                if t_next > best:
-                    best, rho = t_next, nxt[0].to(dev)
+                _, g = self.problem.value_and_grad(rho[None].cpu().numpy())
+                pending = _ascend(rho[None].cpu(), torch.as_tensor(g), self.adjoint_step)[0]
                 self._finetune()
             self.log.append(dict(round=rnd, best=best, surrogate_err=err, fallback=bool(fallback)))
             hist.append(best)

@@ -255,7 +255,7 @@ def run_b200(args):
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": desc, "grid": [ny, nx], "time_steps": n_steps, "step": "one full run",
                        "l2": "flushed (512 MB write) before every run", "parallelism": f"replicas x{world}",
-                       "time_block": tb},
+                       "time_block": tb, "tb_tile": eng.tb_tile, "tile_choice": "autotuned"},
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                          "frac": round(achieved / peak, 4), "traffic": traffic,
                          "note": f"step2d_tb: {tb} steps per launch x {BYTES_PER_CELL_2D} B/cell (algorithmic, "
@@ -437,7 +437,7 @@ def run_surrogate(args):
     net = FNO2d()
     net.flops = 0.0
     t0 = time.perf_counter()
-    losses = train_fno(net, rho, T, epochs=args.epochs)
+    fit = train_fno(net, rho, T, epochs=args.epochs)
     torch.cuda.synchronize()
     t_train = time.perf_counter() - t0
     train_tflops = net.flops / t_train / 1e12
@@ -451,7 +451,7 @@ def run_surrogate(args):
     hist_p, sec_p, _ = plain_adjoint(prob, rho0, args.iterations)
     designs_p = prob.fdtd_designs - d0
     target = hist_p[-1] - 1e-3
-    search = SurrogateSearch(prob, net)
+    search = SurrogateSearch(prob, net, replay=(rho, T))
     d1 = prob.fdtd_designs
     hist_s, sec_s, _ = search.run(rho0, rounds=60, target=target)
     designs_s = prob.fdtd_designs - d1
@@ -475,8 +475,12 @@ def run_surrogate(args):
             "time_to_target_ratio": round(sec_p / sec_s, 2),
             "dataset": {"seconds": round(t_data, 1), "fdtd_gcells_per_s": round(args.samples * cells * n_steps /
                                                                                 t_data / 1e9, 1)},
-            "training": {"seconds": round(t_train, 1), "final_mse": round(losses[-1], 6),
-                         "tensor_tflops": round(train_tflops, 1)}}
+            "training": {"seconds": round(t_train, 1), "best_epoch": fit["best_epoch"],
+                         "val_mae_T": round(min(fit["val"]), 4), "tensor_tflops": round(train_tflops, 1)},
+            "T_stats": {"train_mean": round(float(T.mean()), 4), "train_std": round(float(T.std()), 4),
+                        "train_max": round(float(T.max()), 4)},
+            "rounds_log": [{k: (round(v, 4) if isinstance(v, float) else v) for k, v in r.items()}
+                           for r in search.log]}
     print(json.dumps(line), flush=True)
 
 

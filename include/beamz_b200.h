@@ -397,7 +397,10 @@ int bz_rasterize3d(int32_t nx, int32_t ny, int32_t nz, int32_t n_zs, const doubl
  * across blocks and needs atomic. */
 typedef struct bz_gemm {
   int32_t M, N, K, batch, splitk, act;
-  int32_t ta, tb, atomic, reserved;
+  int32_t ta, tb, atomic;
+  int32_t engine;               /* 0: tcgen05/TMEM kernel where eligible (ta = 0, tb = 1,
+                                   M >= 128, N >= 256, K >= 64, 16-byte aligned rows),
+                                   else mma.sync; 1: mma.sync only */
   const void* A;
   int64_t lda, sa;
   const void* B;
@@ -415,6 +418,10 @@ typedef struct bz_gemm {
 } bz_gemm;
 
 int bz_gemm_bf16(const bz_gemm* g, void* stream);
+
+/* Error word of the tcgen05 GEMM (non-zero: a pipeline wait ran out; that CTA left
+ * its tile unwritten). Synchronous read; reset = 1 clears it. */
+int bz_gemm_error(int32_t* value, int32_t reset);
 
 /* Spectral channel mixing of one Fourier layer, per mode k < n_modes:
  * O[b][o][k] = sum_c U[b][c][k] * W[k][c][o] (complex, (re, im) pairs, bf16). */

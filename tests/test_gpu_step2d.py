@@ -257,3 +257,18 @@ def test_tile_heights_agree(bz, rows):
         sim.run(live=False, save=False, save_memory_mode=True)
         outs.append(sim.engine.field("Ez").cpu().numpy())
     assert rel_l2(outs[1], outs[0]) <= 1e-6
+
+
+def test_autotune_picks_a_candidate_and_keeps_results(bz):
+    from beamz_b200.simulation import engine2d as E
+
+    eps, sigma, dx, dt, t, srcs, mons, freqs = _tiled_problem(bz, seed=29, n_steps=140)
+    outs = []
+    for tb in ("auto", 1):
+        eng = E.Engine2D(eps, sigma, dx, dx, dt, len(t), srcs, mons, precision="fp32", record=True, time_block=tb)
+        eng.run_steps(140)
+        outs.append((eng.field("Ez").cpu().numpy(), eng.take_records(), eng))
+    chosen = (outs[0][2].time_block, outs[0][2].tb_tile)
+    assert chosen in E.TUNE_CANDIDATES
+    np.testing.assert_array_equal(outs[0][0], outs[1][0])
+    np.testing.assert_array_equal(outs[0][1], outs[1][1])

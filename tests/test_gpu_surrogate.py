@@ -140,3 +140,64 @@ def test_transmission_problem_and_search_loop(bz):
     assert all(b >= a for a, b in zip(hist, hist[1:]))
     assert prob.fdtd_designs - before >= 1 + 2 * 4
     assert best.shape == (120, 120) and best.min() >= 0 and best.max() <= 1
+
+
+@pytest.mark.parametrize("M,N,K,batch,split", [(128, 256, 64, 1, 1), (300, 600, 200, 2, 1), (256, 512, 1000, 1, 3)])
+def test_tcgen05_gemm_matches_mma_sync_and_f32(bz, M, N, K, batch, split):
+    """The tcgen05/TMEM kernel (A row-major, B stored [N][K]) against the mma.sync
+    kernel and an f32 matmul of the same bf16 operands: relative L2 <= 1e-5."""
+    from beamz_b200 import _native as nat
+
+    g = torch.Generator().manual_seed(M + N + K)
+    A = torch.randn(batch, M, K, generator=g).to(torch.bfloat16)
+    Bt = torch.randn(batch, N, K, generator=g).to(torch.bfloat16)  # stored [N][K]
+    add = torch.randn(batch, M, N, generator=g)
+    want = torch.bmm(A.float(), Bt.float().transpose(1, 2))
+    dev = "cuda"
+    Ad, Bd, addd = A.to(dev), Bt.to(dev), add.to(dev)
+    outs = {}
+    nat.gemm_error(reset=True)
+    for engine in (0, 1):
+        p = nat.Gemm()
+        p.M, p.N, p.K, p.batch, p.act, p.ta, p.tb, p.engine = M, N, K, batch, 0, 0, 1, engine
+        p.A, p.lda, p.sa = Ad.data_ptr(), K, M * K
+        p.B, p.ldb, p.sb = Bd.data_ptr(), K, N * K
+        p.alpha = 1.0
+        if split == 1:
+            out = torch.empty(batch, M, N, device=dev)
+            p.splitk, p.atomic, p.cadd, p.ldadd, p.sadd = 1, 0, addd.data_ptr(), N, M * N
+        else:
+            out = torch.zeros(batch, M, N, device=dev)
+            p.splitk, p.atomic = split, 1
+        p.outf, p.ldc, p.sc = out.data_ptr(), N, M * N
+        nat.gemm(p, torch.cuda.current_stream().cuda_stream)
+        torch.cuda.synchronize()
+        outs[engine] = out
+    assert nat.gemm_error(reset=True) == 0
+    ref = want + (add if split == 1 else 0)
+    assert rel(outs[0], ref) <= 1e-5
+    assert rel(outs[0], outs[1]) <= 1e-5
+
+
+def test_fno_with_tcgen05_spectral_gemms_matches_oracle(bz):
+    """n = 64, 8 modes, width 32, batch 8: the DFT GEMMs (M = 256, N = 256, K = 4096)
+    and their inverses run on the tcgen05 kernel."""
+    from beamz_b200 import _native as nat
+    from beamz_b200.surrogate.fno import FNO2d
+
+    net = FNO2d(n=64, width=32, modes=8, layers=2, head=16, n_out=5, seed=2)
+    g = torch.Generator().manual_seed(5)
+    rho = torch.rand(8, 64, 64, generator=g, dtype=torch.float64)
+    target = torch.rand(8, 5, generator=g, dtype=torch.float64)
+    out = net.forward(rho.cuda(), keep=True)
+    params = _oracle_params(net)
+    rho_r = rho.clone().requires_grad_(True)
+    ref = fno_ref.forward(params, rho_r, 64, 8, 2)
+    assert rel(out, ref.detach()) <= 3e-2
+    ((ref - target) ** 2).sum().backward()
+    net.zero_grad()
+    d_rho = net.backward((2 * (ref.detach() - target)).float().cuda(), want_input_grad=True)
+    for k, q in net.params.items():
+        assert rel(q.g, params[k].grad) <= 6e-2, (k, rel(q.g, params[k].grad))
+    assert rel(d_rho, rho_r.grad) <= 6e-2
+    assert nat.gemm_error(reset=True) == 0
