@@ -442,66 +442,104 @@ bool tc_eligible(const GemmP& p) {
 }
 
 // ---- spectral channel mixing: O[b][o][k] = sum_c U[b][c][k] * W[k][c][o] (complex) ---
-// U, O: [B][C][n_modes][2] bf16 (re, im); W: [n_modes][Ci][Co][2] bf16.
-__global__ void spectral_fwd_kernel(const bf16* __restrict__ U, const bf16* __restrict__ W, bf16* __restrict__ O,
-                                    int B, int Ci, int Co, int nk) {
+// U, O: [B][C][n_modes][2] bf16 (re, im); W: [n_modes][Ci][Co][2] bf16. One block per
+// mode: the mode's weights and a chunk of SB designs' coefficients are staged in shared
+// memory (as float2), then every thread forms whole output sums from there.
+constexpr int SB = 64;     // designs per shared-memory chunk
+constexpr int SMAXC = 32;  // channels supported by the staged kernels
+
+__device__ __forceinline__ float2 ld_c(const bf16* p) {
+  return make_float2(__bfloat162float(p[0]), __bfloat162float(p[1]));
+}
+
+__global__ void __launch_bounds__(256) spectral_fwd_kernel(const bf16* __restrict__ U, const bf16* __restrict__ W,
+                                                           bf16* __restrict__ O, int B, int Ci, int Co, int nk) {
+  __shared__ float2 sw[SMAXC * SMAXC];
+  __shared__ float2 su[SB * SMAXC];
   const int k = blockIdx.x;
-  const int o = threadIdx.x;  // Co threads
-  const bf16* w = W + (long long)k * Ci * Co * 2;
-  for (int b = blockIdx.y; b < B; b += gridDim.y) {
-    float re = 0.f, im = 0.f;
-    for (int c = 0; c < Ci; ++c) {
-      const long long ui = (((long long)b * Ci + c) * nk + k) * 2;
-      const float ur = __bfloat162float(U[ui]), uim = __bfloat162float(U[ui + 1]);
-      const float wr = __bfloat162float(w[(c * Co + o) * 2]), wi = __bfloat162float(w[(c * Co + o) * 2 + 1]);
-      re = fmaf(ur, wr, fmaf(-uim, wi, re));
-      im = fmaf(ur, wi, fmaf(uim, wr, im));
+  for (int t = threadIdx.x; t < Ci * Co; t += blockDim.x) sw[t] = ld_c(W + ((long long)k * Ci * Co + t) * 2);
+  for (int b0 = 0; b0 < B; b0 += SB) {
+    const int nb = min(SB, B - b0);
+    __syncthreads();
+    for (int t = threadIdx.x; t < nb * Ci; t += blockDim.x) {
+      const int b = t / Ci, c = t - b * Ci;
+      su[t] = ld_c(U + (((long long)(b0 + b) * Ci + c) * nk + k) * 2);
     }
-    const long long oi = (((long long)b * Co + o) * nk + k) * 2;
-    O[oi] = __float2bfloat16_rn(re);
-    O[oi + 1] = __float2bfloat16_rn(im);
+    __syncthreads();
+    for (int t = threadIdx.x; t < nb * Co; t += blockDim.x) {
+      const int b = t / Co, o = t - b * Co;
+      float re = 0.f, im = 0.f;
+      for (int c = 0; c < Ci; ++c) {
+        const float2 u = su[b * Ci + c], w = sw[c * Co + o];
+        re = fmaf(u.x, w.x, fmaf(-u.y, w.y, re));
+        im = fmaf(u.x, w.y, fmaf(u.y, w.x, im));
+      }
+      bf16* q = O + (((long long)(b0 + b) * Co + o) * nk + k) * 2;
+      q[0] = __float2bfloat16_rn(re);
+      q[1] = __float2bfloat16_rn(im);
+    }
   }
 }
 
-// dU[b][c][k] = sum_o dO[b][o][k] * conj(W[k][c][o]); thread per c.
-__global__ void spectral_bwd_u_kernel(const bf16* __restrict__ dO, const bf16* __restrict__ W, bf16* __restrict__ dU,
-                                      int B, int Ci, int Co, int nk) {
+// Backward of one mode: dU[b][c] = sum_o dO[b][o] conj(W[c][o]); dW[c][o] += sum_b dO[b][o]
+// conj(U[b][c]) (f32).
+__global__ void __launch_bounds__(256) spectral_bwd_kernel(const bf16* __restrict__ dO, const bf16* __restrict__ U,
+                                                           const bf16* __restrict__ W, bf16* __restrict__ dU,
+                                                           float* __restrict__ dW, int B, int Ci, int Co, int nk) {
+  __shared__ float2 sw[SMAXC * SMAXC];
+  __shared__ float2 su[SB * SMAXC];
+  __shared__ float2 sg[SB * SMAXC];
   const int k = blockIdx.x;
-  const int c = threadIdx.x;
-  const bf16* w = W + (long long)k * Ci * Co * 2;
-  for (int b = blockIdx.y; b < B; b += gridDim.y) {
-    float re = 0.f, im = 0.f;
-    for (int o = 0; o < Co; ++o) {
-      const long long gi = (((long long)b * Co + o) * nk + k) * 2;
-      const float gr = __bfloat162float(dO[gi]), gim = __bfloat162float(dO[gi + 1]);
-      const float wr = __bfloat162float(w[(c * Co + o) * 2]), wi = __bfloat162float(w[(c * Co + o) * 2 + 1]);
-      re = fmaf(gr, wr, fmaf(gim, wi, re));
-      im = fmaf(gim, wr, fmaf(-gr, wi, im));
+  for (int t = threadIdx.x; t < Ci * Co; t += blockDim.x) sw[t] = ld_c(W + ((long long)k * Ci * Co + t) * 2);
+  // each thread owns (c, o) pairs t, t + blockDim, ... of dW
+  float2 acc[(SMAXC * SMAXC + 255) / 256];
+#pragma unroll
+  for (int i = 0; i < (SMAXC * SMAXC + 255) / 256; ++i) acc[i] = make_float2(0.f, 0.f);
+  for (int b0 = 0; b0 < B; b0 += SB) {
+    const int nb = min(SB, B - b0);
+    __syncthreads();
+    for (int t = threadIdx.x; t < nb * Ci; t += blockDim.x) {
+      const int b = t / Ci, c = t - b * Ci;
+      su[t] = ld_c(U + (((long long)(b0 + b) * Ci + c) * nk + k) * 2);
     }
-    const long long ui = (((long long)b * Ci + c) * nk + k) * 2;
-    dU[ui] = __float2bfloat16_rn(re);
-    dU[ui + 1] = __float2bfloat16_rn(im);
+    for (int t = threadIdx.x; t < nb * Co; t += blockDim.x) {
+      const int b = t / Co, o = t - b * Co;
+      sg[t] = ld_c(dO + (((long long)(b0 + b) * Co + o) * nk + k) * 2);
+    }
+    __syncthreads();
+    for (int t = threadIdx.x; t < nb * Ci; t += blockDim.x) {
+      const int b = t / Ci, c = t - b * Ci;
+      float re = 0.f, im = 0.f;
+      for (int o = 0; o < Co; ++o) {
+        const float2 g = sg[b * Co + o], w = sw[c * Co + o];
+        re = fmaf(g.x, w.x, fmaf(g.y, w.y, re));
+        im = fmaf(g.y, w.x, fmaf(-g.x, w.y, im));
+      }
+      bf16* q = dU + (((long long)(b0 + b) * Ci + c) * nk + k) * 2;
+      q[0] = __float2bfloat16_rn(re);
+      q[1] = __float2bfloat16_rn(im);
+    }
+#pragma unroll
+    for (int i = 0; i < (SMAXC * SMAXC + 255) / 256; ++i) {
+      const int t = threadIdx.x + i * 256;
+      if (t >= Ci * Co) break;
+      const int c = t / Co, o = t - c * Co;
+      float2 a = acc[i];
+      for (int b = 0; b < nb; ++b) {
+        const float2 g = sg[b * Co + o], u = su[b * Ci + c];
+        a.x = fmaf(g.x, u.x, fmaf(g.y, u.y, a.x));
+        a.y = fmaf(g.y, u.x, fmaf(-g.x, u.y, a.y));
+      }
+      acc[i] = a;
+    }
   }
-}
-
-// dW[k][c][o] += sum_b dO[b][o][k] * conj(U[b][c][k]) (f32); thread per (c, o).
-__global__ void spectral_bwd_w_kernel(const bf16* __restrict__ dO, const bf16* __restrict__ U, float* __restrict__ dW,
-                                      int B, int Ci, int Co, int nk) {
-  const int k = blockIdx.x;
-  for (int t = threadIdx.x; t < Ci * Co; t += blockDim.x) {
-    const int c = t / Co, o = t % Co;
-    float re = 0.f, im = 0.f;
-    for (int b = 0; b < B; ++b) {
-      const long long gi = (((long long)b * Co + o) * nk + k) * 2;
-      const long long ui = (((long long)b * Ci + c) * nk + k) * 2;
-      const float gr = __bfloat162float(dO[gi]), gim = __bfloat162float(dO[gi + 1]);
-      const float ur = __bfloat162float(U[ui]), uim = __bfloat162float(U[ui + 1]);
-      re = fmaf(gr, ur, fmaf(gim, uim, re));
-      im = fmaf(gim, ur, fmaf(-gr, uim, im));
-    }
-    float* d = dW + (((long long)k * Ci + c) * Co + o) * 2;
-    d[0] += re;
-    d[1] += im;
+#pragma unroll
+  for (int i = 0; i < (SMAXC * SMAXC + 255) / 256; ++i) {
+    const int t = threadIdx.x + i * 256;
+    if (t >= Ci * Co) break;
+    float* d = dW + ((long long)k * Ci * Co + t) * 2;
+    d[0] += acc[i].x;
+    d[1] += acc[i].y;
   }
 }
 
@@ -523,12 +561,13 @@ __global__ void row_mean_kernel(const bf16* __restrict__ x, float* __restrict__ 
   if (lane == 0) out[r] = s * scale;
 }
 
-// Sum over rows: out[c] += sum_{b} sum_p x[b][c][p] (bf16 in, f32 out); block per (c).
+// Sum over rows: out[c] += sum_b sum_p x[b][c][p] (bf16 in, f32 out); one block per
+// (c, b) row of P values, reduced in the block and added atomically.
 __global__ void chan_sum_kernel(const bf16* __restrict__ x, float* __restrict__ out, int B, int C, int P) {
-  const int c = blockIdx.x;
+  const int c = blockIdx.x, b = blockIdx.y;
+  const bf16* row = x + ((long long)b * C + c) * P;
   float s = 0.f;
-  for (int b = 0; b < B; ++b)
-    for (int p = threadIdx.x; p < P; p += blockDim.x) s += __bfloat162float(x[((long long)b * C + c) * P + p]);
+  for (int p = threadIdx.x; p < P; p += blockDim.x) s += __bfloat162float(row[p]);
   __shared__ float red[32];
   for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
   if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
@@ -536,7 +575,7 @@ __global__ void chan_sum_kernel(const bf16* __restrict__ x, float* __restrict__ 
   if (threadIdx.x < 32) {
     s = threadIdx.x < (int)(blockDim.x >> 5) ? red[threadIdx.x] : 0.f;
     for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-    if (threadIdx.x == 0) out[c] += s;
+    if (threadIdx.x == 0) atomicAdd(out + c, s);
   }
 }
 
@@ -624,25 +663,20 @@ extern "C" int bz_gemm_error(int32_t* value, int32_t reset) {
 extern "C" int bz_spectral_mix(const void* U, const void* W, void* O, int32_t B, int32_t ci, int32_t co,
                                int32_t n_modes, void* stream) {
   BZ_REQUIRE(U && W && O, "bz_spectral_mix: NULL buffer");
-  BZ_REQUIRE(B >= 1 && ci >= 1 && co >= 1 && co <= 1024 && n_modes >= 1, "bz_spectral_mix: bad sizes");
-  dim3 grid((unsigned)n_modes, (unsigned)(B < 64 ? B : 64));
-  bz::spectral_fwd_kernel<<<grid, co, 0, bz::as_stream(stream)>>>((const bz::bf16*)U, (const bz::bf16*)W,
-                                                                     (bz::bf16*)O, B, ci, co, n_modes);
+  BZ_REQUIRE(B >= 1 && ci >= 1 && co >= 1 && ci <= bz::SMAXC && co <= bz::SMAXC && n_modes >= 1,
+             "bz_spectral_mix: bad sizes (channels up to %d)", bz::SMAXC);
+  bz::spectral_fwd_kernel<<<(unsigned)n_modes, 256, 0, bz::as_stream(stream)>>>(
+      (const bz::bf16*)U, (const bz::bf16*)W, (bz::bf16*)O, B, ci, co, n_modes);
   return bz::check_launch("bz_spectral_mix");
 }
 
 extern "C" int bz_spectral_mix_bwd(const void* dO, const void* U, const void* W, void* dU, float* dW, int32_t B,
                                    int32_t ci, int32_t co, int32_t n_modes, void* stream) {
   BZ_REQUIRE(dO && U && W && dU && dW, "bz_spectral_mix_bwd: NULL buffer");
-  BZ_REQUIRE(B >= 1 && ci >= 1 && ci <= 1024 && co >= 1 && n_modes >= 1, "bz_spectral_mix_bwd: bad sizes");
-  cudaStream_t st = bz::as_stream(stream);
-  dim3 grid((unsigned)n_modes, (unsigned)(B < 64 ? B : 64));
-  bz::spectral_bwd_u_kernel<<<grid, ci, 0, st>>>((const bz::bf16*)dO, (const bz::bf16*)W, (bz::bf16*)dU, B, ci, co,
-                                                 n_modes);
-  int rc = bz::check_launch("bz_spectral_mix_bwd");
-  if (rc != BZ_OK) return rc;
-  bz::spectral_bwd_w_kernel<<<(unsigned)n_modes, 256, 0, st>>>((const bz::bf16*)dO, (const bz::bf16*)U, dW, B, ci,
-                                                               co, n_modes);
+  BZ_REQUIRE(B >= 1 && ci >= 1 && co >= 1 && ci <= bz::SMAXC && co <= bz::SMAXC && n_modes >= 1,
+             "bz_spectral_mix_bwd: bad sizes (channels up to %d)", bz::SMAXC);
+  bz::spectral_bwd_kernel<<<(unsigned)n_modes, 256, 0, bz::as_stream(stream)>>>(
+      (const bz::bf16*)dO, (const bz::bf16*)U, (const bz::bf16*)W, (bz::bf16*)dU, dW, B, ci, co, n_modes);
   return bz::check_launch("bz_spectral_mix_bwd");
 }
 
@@ -672,7 +706,9 @@ extern "C" int bz_row_broadcast(const float* g, void* x, int64_t rows, int32_t P
 
 extern "C" int bz_chan_sum(const void* x, float* out, int32_t B, int32_t C, int32_t P, void* stream) {
   BZ_REQUIRE(x && out && B >= 1 && C >= 1 && P >= 1, "bz_chan_sum: bad arguments");
-  bz::chan_sum_kernel<<<(unsigned)C, 256, 0, bz::as_stream(stream)>>>((const bz::bf16*)x, out, B, C, P);
+  BZ_REQUIRE(B <= 65535, "bz_chan_sum: B above 65535");
+  bz::chan_sum_kernel<<<dim3((unsigned)C, (unsigned)B), 256, 0, bz::as_stream(stream)>>>((const bz::bf16*)x, out, B,
+                                                                                        C, P);
   return bz::check_launch("bz_chan_sum");
 }
 

@@ -571,8 +571,9 @@ int launch_tb(const bz_grid2d* gd, const bz_fields2d* f, const bz_source_ops* s,
   return check_launch("bz_step2d_multi");
 }
 
-// Tile shapes: 1 = 4 rows x 8 warps, 2 = 4 rows x 16 warps, 3 = 8 rows x 8 warps
-// (float, one component); wider types use 2 rows x 16 warps.
+// Tile shapes: 1 = 4 rows x 8 warps, 2 = 4 rows x 16 warps, 3 = 8 rows x 8 warps,
+// 4 = 5 rows x 16 warps, 5 = 6 rows x 12 warps (float, one component); wider types
+// use 2 rows x 16 warps.
 template <typename T, int NC, int TS>
 int tb_by_tile(const bz_grid2d* g, const bz_fields2d* f, const bz_source_ops* s, const bz_monitor_ops* m,
                int64_t step, int32_t tile, const int64_t* d_step, cudaStream_t st) {
@@ -580,6 +581,8 @@ int tb_by_tile(const bz_grid2d* g, const bz_fields2d* f, const bz_source_ops* s,
     switch (tile) {
       case 1: return launch_tb<T, NC, TS, 4, 8>(g, f, s, m, step, d_step, st);
       case 3: return launch_tb<T, NC, TS, 8, 8>(g, f, s, m, step, d_step, st);
+      case 4: return launch_tb<T, NC, TS, 5, 16>(g, f, s, m, step, d_step, st);
+      case 5: return launch_tb<T, NC, TS, 6, 12>(g, f, s, m, step, d_step, st);
       default: return launch_tb<T, NC, TS, 4, 16>(g, f, s, m, step, d_step, st);
     }
   } else {
@@ -691,7 +694,7 @@ extern "C" int bz_step2d_multi(const bz_grid2d* g, const bz_fields2d* f, const b
   if (rc != BZ_OK) return rc;
   BZ_REQUIRE(n_sub == 1 || n_sub == 3 || n_sub == 5 || n_sub == 7, "bz_step2d_multi: n_sub must be 1, 3, 5 or 7 (got %d)",
              n_sub);
-  BZ_REQUIRE(tile >= 0 && tile <= 3, "bz_step2d_multi: tile must be 0..3 (got %d)", tile);
+  BZ_REQUIRE(tile >= 0 && tile <= 5, "bz_step2d_multi: tile must be 0..5 (got %d)", tile);
   if (n_sub == 1) return bz_step2d(g, f, s, m, step, d_step, stream);
   if (f->power != nullptr || (m && m->region != nullptr))
     return bz::fail(BZ_ERR_UNSUPPORTED, "bz_step2d_multi: power accumulation and region capture need bz_step2d");

@@ -21,7 +21,7 @@ from .compile_ops import SourceOps, compile_monitors_2d, compile_sources
 GRAPH_CHUNK = 64  # at most this many steps per captured graph
 RING_LEN = GRAPH_CHUNK  # monitor samples kept between DFT folds
 # (steps per launch, register-tile shape) tried by the autotuner
-TUNE_CANDIDATES = ((7, 0), (7, 1), (7, 3), (5, 0), (5, 1), (3, 1))
+TUNE_CANDIDATES = ((7, 0), (7, 4), (7, 5), (7, 1), (7, 3), (5, 0), (5, 4), (5, 1), (3, 1))
 _TUNED: dict = {}  # (device name, nx, ny, designs, components, dtype) -> (time_block, tb_tile)
 
 
@@ -266,26 +266,31 @@ class Engine2D:
             self._graphs[phase] = g
         return g
 
-    def autotune(self, candidates=TUNE_CANDIDATES, launches: int = 4):
+    def autotune(self, candidates=TUNE_CANDIDATES, launches: int = 12, rounds: int = 2):
         """Pick (time_block, tb_tile) by timing blocked launches on this grid (CUDA events).
 
         Every candidate gives the same results (same arithmetic per cell), and a launch
         only writes the copy that the next step overwrites and ring/record slots of steps
-        not yet taken, so timing from the current state changes nothing. The choice is
-        cached per (device, grid, designs, components, dtype) for the process."""
+        not yet taken, so timing from the current state changes nothing. Each candidate
+        is launched once to warm up, then timed over ``launches`` launches in ``rounds``
+        interleaved rounds (best time kept). The choice is cached per (device, grid,
+        designs, components, dtype) for the process."""
         key = (torch.cuda.get_device_name(self.dev), self.nx, self.ny, self.n_designs, self.n_comp, self.bz_dtype)
         if key not in _TUNED:
-            times = {}
+            times = {c: float("inf") for c in candidates}
             for tb, tile in candidates:
                 self.time_block, self.tb_tile = tb, tile
-                self._launch_tb(self.step_index, None)  # warm-up
-                a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-                a.record()
-                for _ in range(launches):
-                    self._launch_tb(self.step_index, None)
-                b.record()
-                b.synchronize()
-                times[(tb, tile)] = a.elapsed_time(b) / (launches * tb)
+                self._launch_tb(self.step_index, None)
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            for _ in range(rounds):
+                for tb, tile in candidates:
+                    self.time_block, self.tb_tile = tb, tile
+                    a.record()
+                    for _ in range(launches):
+                        self._launch_tb(self.step_index, None)
+                    b.record()
+                    b.synchronize()
+                    times[(tb, tile)] = min(times[(tb, tile)], a.elapsed_time(b) / (launches * tb))
             _TUNED[key] = min(times, key=times.get)
             self.tune_times = times
         self.time_block, self.tb_tile = _TUNED[key]

@@ -255,7 +255,9 @@ def run_b200(args):
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": desc, "grid": [ny, nx], "time_steps": n_steps, "step": "one full run",
                        "l2": "flushed (512 MB write) before every run", "parallelism": f"replicas x{world}",
-                       "time_block": tb, "tb_tile": eng.tb_tile, "tile_choice": "autotuned"},
+                       "time_block": tb, "tb_tile": eng.tb_tile, "tile_choice": "autotuned",
+                       "tune_us_per_step": {f"{k[0]}/{k[1]}": round(v * 1e3, 3)
+                                            for k, v in getattr(eng, "tune_times", {}).items()}},
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                          "frac": round(achieved / peak, 4), "traffic": traffic,
                          "note": f"step2d_tb: {tb} steps per launch x {BYTES_PER_CELL_2D} B/cell (algorithmic, "

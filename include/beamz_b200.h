@@ -153,9 +153,9 @@ int bz_step2d(const bz_grid2d* g, const bz_fields2d* f, const bz_source_ops* src
  * monitor records and ring samples per sub-step). Each block keeps a tile of the
  * grid in registers for all sub-steps and stores the part of it that stays exact.
  * n_sub: 1, 3, 5 or 7 (odd, so the copy read stays (step & 1) and the result lands
- * in copy ((step + n_sub) & 1)); 1 is bz_step2d. tile: 0 = default, 1..3 = tile
- * shapes of 4x8, 4x16 and 8x8 (rows per warp x warps) for float32 single-component
- * fields. Power accumulation and region capture return BZ_ERR_UNSUPPORTED (use
+ * in copy ((step + n_sub) & 1)); 1 is bz_step2d. tile: 0 = default (4x16), 1..5 =
+ * tile shapes of 4x8, 4x16, 8x8, 5x16 and 6x12 (rows per warp x warps) for float32
+ * single-component fields. Power accumulation and region capture return BZ_ERR_UNSUPPORTED (use
  * bz_step2d for those steps). */
 int bz_step2d_multi(const bz_grid2d* g, const bz_fields2d* f, const bz_source_ops* src,
                     const bz_monitor_ops* mon, int64_t step, int32_t n_sub, int32_t tile,
@@ -424,7 +424,8 @@ int bz_gemm_bf16(const bz_gemm* g, void* stream);
 int bz_gemm_error(int32_t* value, int32_t reset);
 
 /* Spectral channel mixing of one Fourier layer, per mode k < n_modes:
- * O[b][o][k] = sum_c U[b][c][k] * W[k][c][o] (complex, (re, im) pairs, bf16). */
+ * O[b][o][k] = sum_c U[b][c][k] * W[k][c][o] (complex, (re, im) pairs, bf16);
+ * ci, co <= 32. */
 int bz_spectral_mix(const void* U, const void* W, void* O, int32_t B, int32_t ci, int32_t co, int32_t n_modes,
                     void* stream);
 /* Its backward: dU = sum_o dO * conj(W); dW (f32, accumulated) += sum_b dO * conj(U). */
