@@ -11,7 +11,10 @@
 // mma.sync.m16n8k16 (bf16 inputs, f32 accumulators). The epilogue adds an f32
 // term, row/column biases, applies GELU, and stores f32 and/or bf16, or
 // accumulates atomically (batch-reduced or split-K weight gradients).
+#include <cuda.h>
 #include <cuda_bf16.h>
+
+#include <mutex>
 
 #include "bz_internal.cuh"
 
@@ -435,6 +438,204 @@ int launch_gemm_tc(const GemmP& p, cudaStream_t st) {
   return check_launch("bz_gemm_bf16");
 }
 
+
+// ---- tcgen05 + TMA path (batch 1): one control thread, four-stage pipeline --------
+// Operand stages are filled by TMA tiled copies (2D tensor maps over the row-major
+// K-contiguous A and B, box 8 elements x rows: each copy writes one 8-element K chunk
+// of 128 (A) or 256 (B) rows, i.e. one column of no-swizzle K-major core matrices).
+// Thread 0 waits for a stage's copies (mbarrier complete_tx), issues its two MMAs,
+// commits them to the stage's "empty" barrier, and refills the previous stage once its
+// MMAs are done, so the tensor pipe always has queued work. 96 KB of stages: two CTAs
+// per SM, one's epilogue overlapping the other's main loop. Bounded waits as above.
+namespace tma {
+constexpr int S = 4, BK = 32;
+constexpr int A_ST = tc::BM * BK * 2, B_ST = tc::BN * BK * 2, STAGE = A_ST + B_ST;
+constexpr int LBO_A = tc::BM * 16, LBO_B = tc::BN * 16;  // bytes between K chunks
+constexpr int SMEM = S * STAGE + 1024 + 128;             // + alignment slack + barriers
+}  // namespace tma
+
+__device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap* map, int x, int y, uint32_t mbar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];\n" ::"r"(
+          dst),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(mbar)
+      : "memory");
+}
+
+__global__ void __launch_bounds__(tc::THREADS) gemm_tma_kernel(const __grid_constant__ CUtensorMap tmA,
+                                                                const __grid_constant__ CUtensorMap tmB, GemmP p) {
+  extern __shared__ unsigned char smem_raw[];
+  unsigned char* smem = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int ks = blockIdx.z;
+  const int m0 = blockIdx.y * tc::BM, n0 = blockIdx.x * tc::BN;
+  const int ktiles = (p.K + tma::BK - 1) / tma::BK;
+  const int kper = (ktiles + p.splitk - 1) / p.splitk;
+  const int kt0 = ks * kper, kt1 = min(ktiles, kt0 + kper);
+  const int nt = max(0, kt1 - kt0);
+  unsigned char* bar = smem + tma::S * tma::STAGE;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bar + 8 * (2 * tma::S + 1));
+  const uint32_t sbase = static_cast<uint32_t>(__cvta_generic_to_shared(smem));
+  const uint32_t full0 = static_cast<uint32_t>(__cvta_generic_to_shared(bar));
+  const uint32_t empty0 = full0 + 8 * tma::S, done = full0 + 16 * tma::S;
+
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(
+                     static_cast<uint32_t>(__cvta_generic_to_shared(tmem_slot))),
+                 "r"(tc::BN));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::);
+  }
+  if (tid == 0) {
+    for (int i = 0; i < 2 * tma::S + 1; ++i) asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(full0 + 8 * i));
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;\n" ::);
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
+  const uint32_t taddr = *tmem_slot;
+
+  int ok = 1;
+  if (tid == 0 && nt > 0) {
+    auto issue = [&](int t) {  // tile kt0 + t into stage t % S
+      const int s = t % tma::S, k0 = (kt0 + t) * tma::BK;
+      const uint32_t st = sbase + s * tma::STAGE, fb = full0 + 8 * s;
+      asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(fb), "r"(tma::STAGE) : "memory");
+#pragma unroll
+      for (int j = 0; j < tma::BK / 8; ++j) {
+        tma_load_2d(st + j * tma::LBO_A, &tmA, k0 + 8 * j, m0, fb);
+        tma_load_2d(st + tma::A_ST + j * tma::LBO_B, &tmB, k0 + 8 * j, n0, fb);
+      }
+    };
+    int issued = 0, consumed = 0;
+    for (; issued < min(tma::S, nt); ++issued) issue(issued);
+    for (int it = 0; it < nt; ++it) {
+      const int s = it % tma::S;
+      if (!tc_wait(full0 + 8 * s, (uint32_t)((it / tma::S) & 1))) {
+        ok = 0;
+        break;
+      }
+      consumed = it + 1;
+      asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
+      const uint32_t a0 = sbase + s * tma::STAGE, b0 = a0 + tma::A_ST;
+#pragma unroll
+      for (int kk = 0; kk < tma::BK / 16; ++kk) {
+        const uint64_t da = tc_sdesc(a0 + kk * 2 * tma::LBO_A, tma::LBO_A, 128);
+        const uint64_t db = tc_sdesc(b0 + kk * 2 * tma::LBO_B, tma::LBO_B, 128);
+        const uint32_t acc = (it > 0 || kk > 0) ? 1u : 0u;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+            "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n"
+            :
+            : "r"(taddr), "l"(da), "l"(db), "r"(tc::IDESC), "r"(acc), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
+      }
+      asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(
+          empty0 + 8 * s));
+      if (it >= 1 && issued < nt) {  // refill the previous stage once its MMAs are done
+        const int sp = (it - 1) % tma::S;
+        if (!tc_wait(empty0 + 8 * sp, (uint32_t)(((it - 1) / tma::S) & 1))) {
+          ok = 0;
+          break;
+        }
+        issue(issued++);
+      }
+    }
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(done));
+    for (int t = consumed; t < issued; ++t)  // copies still in flight after a failure
+      tc_wait(full0 + 8 * (t % tma::S), (uint32_t)((t / tma::S) & 1));
+  }
+  ok = __syncthreads_and(ok);
+  if (nt > 0) {
+    if (!tc_wait(done, 0u)) ok = 0;
+  }
+  ok = __syncthreads_and(ok);
+  if (!ok && tid == 0) atomicExch(&g_tc_error, 1);
+  asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
+  const int m = m0 + warp * 32 + lane;
+  if (ok) {
+    for (int c0 = 0; c0 < tc::BN; c0 += 8) {
+      uint32_t v[8];
+      if (nt > 0) {
+        asm volatile(
+            "tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];\n"
+            : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7])
+            : "r"(taddr + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0));
+        asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+      } else {
+#pragma unroll
+        for (int e = 0; e < 8; ++e) v[e] = 0u;
+      }
+#pragma unroll
+      for (int e = 0; e < 8; ++e) {
+        const int n = n0 + c0 + e;
+        if (m >= p.M || n >= p.N) continue;
+        float x = p.alpha * __uint_as_float(v[e]);
+        if (p.cadd) x += p.cadd[(long long)m * p.ldadd + n];
+        if (p.bias_m) x += p.bias_m[m];
+        if (p.bias_n) x += p.bias_n[n];
+        if (p.pre) p.pre[(long long)m * p.ldpre + n] = __float2bfloat16_rn(x);
+        if (p.act == 1) x = gelu_f(x);
+        const long long o = (long long)m * p.ldc + n;
+        if (p.outf) {
+          if (p.atomic) atomicAdd(p.outf + o, x); else p.outf[o] = x;
+        }
+        if (p.outh) p.outh[o] = __float2bfloat16_rn(x);
+      }
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;\n" ::);
+  __syncthreads();
+  if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(taddr), "r"(tc::BN));
+}
+
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiledFn encode_fn() {
+  static std::once_flag once;
+  static EncodeTiledFn fn = nullptr;
+  std::call_once(once, [] {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<EncodeTiledFn>(f);
+  });
+  return fn;
+}
+
+// 2D map over a row-major bf16 matrix of `rows` x `cols` (cols contiguous, ld elements
+// per row), box 8 columns x box_rows rows; out-of-range elements read as zero.
+bool make_map(CUtensorMap* map, const bf16* base, long long rows, long long cols, long long ld, int box_rows) {
+  EncodeTiledFn fn = encode_fn();
+  if (!fn) return false;
+  const cuuint64_t dim[2] = {(cuuint64_t)cols, (cuuint64_t)rows};
+  const cuuint64_t stride[1] = {(cuuint64_t)ld * 2};
+  const cuuint32_t box[2] = {8u, (cuuint32_t)box_rows};
+  const cuuint32_t estride[2] = {1u, 1u};
+  return fn(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<bf16*>(base), dim, stride, box, estride,
+            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+// 1: launched; 0: not applicable here (caller uses another kernel); <0: error status.
+int launch_gemm_tma(const GemmP& p, cudaStream_t st) {
+  if (p.batch != 1) return 0;
+  alignas(64) CUtensorMap ma, mb;
+  if (!make_map(&ma, p.A, p.M, p.K, p.lda, tc::BM) || !make_map(&mb, p.B, p.N, p.K, p.ldb, tc::BN)) return 0;
+  static bool configured = false;
+  if (!configured) {
+    if (cudaFuncSetAttribute(gemm_tma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, tma::SMEM) != cudaSuccess)
+      return fail(BZ_ERR_CUDA, "bz_gemm_bf16: cannot configure the TMA kernel's shared memory");
+    configured = true;
+  }
+  dim3 grid((unsigned)ceil_div(p.N, tc::BN), (unsigned)ceil_div(p.M, tc::BM), (unsigned)p.splitk);
+  gemm_tma_kernel<<<grid, tc::THREADS, tma::SMEM, st>>>(ma, mb, p);
+  const int rc = check_launch("bz_gemm_bf16");
+  return rc == BZ_OK ? 1 : rc;
+}
+
 bool tc_eligible(const GemmP& p) {
   auto al = [](const void* q) { return (reinterpret_cast<uintptr_t>(q) & 15u) == 0u; };
   return !p.ta && p.tb && p.M >= 128 && p.N >= 256 && p.K >= 64 && p.lda % 8 == 0 && p.ldb % 8 == 0 &&
@@ -640,7 +841,12 @@ extern "C" int bz_gemm_bf16(const bz_gemm* g, void* stream) {
   p.outf = g->outf; p.outh = (bz::bf16*)g->outh; p.ldc = g->ldc; p.sc = g->sc;
   p.pre = (bz::bf16*)g->pre; p.ldpre = g->ldpre; p.spre = g->spre;
   cudaStream_t st = bz::as_stream(stream);
-  if (g->engine == 0 && bz::tc_eligible(p)) return bz::launch_gemm_tc(p, st);
+  if (g->engine == 0 && bz::tc_eligible(p)) {
+    const int t = bz::launch_gemm_tma(p, st);
+    if (t != 0) return t > 0 ? BZ_OK : t;
+    return bz::launch_gemm_tc(p, st);
+  }
+  if (g->engine == 2 && bz::tc_eligible(p)) return bz::launch_gemm_tc(p, st);
   if (g->N <= 32) return bz::launch_gemm<128, 32, 4, 1>(p, st);
   if (g->M <= 32) return bz::launch_gemm<32, 128, 1, 4>(p, st);
   return bz::launch_gemm<128, 128, 2, 4>(p, st);

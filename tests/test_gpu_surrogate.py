@@ -142,10 +142,12 @@ def test_transmission_problem_and_search_loop(bz):
     assert best.shape == (120, 120) and best.min() >= 0 and best.max() <= 1
 
 
-@pytest.mark.parametrize("M,N,K,batch,split", [(128, 256, 64, 1, 1), (300, 600, 200, 2, 1), (256, 512, 1000, 1, 3)])
+@pytest.mark.parametrize("M,N,K,batch,split", [(128, 256, 64, 1, 1), (300, 600, 200, 2, 1), (256, 512, 1000, 1, 3),
+                                                (333, 700, 520, 1, 1)])
 def test_tcgen05_gemm_matches_mma_sync_and_f32(bz, M, N, K, batch, split):
-    """The tcgen05/TMEM kernel (A row-major, B stored [N][K]) against the mma.sync
-    kernel and an f32 matmul of the same bf16 operands: relative L2 <= 1e-5."""
+    """The tcgen05/TMEM kernels (A row-major, B stored [N][K]; engine 0 = TMA-fed for
+    batch 1, engine 2 = register-staged) against the mma.sync kernel (engine 1) and an
+    f32 matmul of the same bf16 operands: relative L2 <= 1e-5."""
     from beamz_b200 import _native as nat
 
     g = torch.Generator().manual_seed(M + N + K)
@@ -157,7 +159,7 @@ def test_tcgen05_gemm_matches_mma_sync_and_f32(bz, M, N, K, batch, split):
     Ad, Bd, addd = A.to(dev), Bt.to(dev), add.to(dev)
     outs = {}
     nat.gemm_error(reset=True)
-    for engine in (0, 1):
+    for engine in (0, 1, 2):
         p = nat.Gemm()
         p.M, p.N, p.K, p.batch, p.act, p.ta, p.tb, p.engine = M, N, K, batch, 0, 0, 1, engine
         p.A, p.lda, p.sa = Ad.data_ptr(), K, M * K
@@ -175,8 +177,9 @@ def test_tcgen05_gemm_matches_mma_sync_and_f32(bz, M, N, K, batch, split):
         outs[engine] = out
     assert nat.gemm_error(reset=True) == 0
     ref = want + (add if split == 1 else 0)
-    assert rel(outs[0], ref) <= 1e-5
-    assert rel(outs[0], outs[1]) <= 1e-5
+    for engine in (0, 2):
+        assert rel(outs[engine], ref) <= 1e-5, engine
+        assert rel(outs[engine], outs[1]) <= 1e-5, engine
 
 
 def test_fno_with_tcgen05_spectral_gemms_matches_oracle(bz):
