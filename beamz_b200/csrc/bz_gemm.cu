@@ -439,20 +439,32 @@ int launch_gemm_tc(const GemmP& p, cudaStream_t st) {
 }
 
 
-// ---- tcgen05 + TMA path (batch 1): one control thread, four-stage pipeline --------
-// Operand stages are filled by TMA tiled copies (2D tensor maps over the row-major
-// K-contiguous A and B, box 8 elements x rows: each copy writes one 8-element K chunk
-// of 128 (A) or 256 (B) rows, i.e. one column of no-swizzle K-major core matrices).
-// Thread 0 waits for a stage's copies (mbarrier complete_tx), issues its two MMAs,
-// commits them to the stage's "empty" barrier, and refills the previous stage once its
-// MMAs are done, so the tensor pipe always has queued work. 96 KB of stages: two CTAs
-// per SM, one's epilogue overlapping the other's main loop. Bounded waits as above.
+// ---- tcgen05 + TMA path (batch 1): one control thread, two-stage pipeline ---------
+// Operand stages are filled by TMA tiled copies with 128-byte swizzling (2D tensor
+// maps over the row-major K-contiguous A and B, box 64 elements x 128 or 256 rows: one
+// copy per operand per stage), which is the K-major SWIZZLE_128B layout of the MMA
+// descriptors (8-row atoms of 128-byte rows, atoms 1024 bytes apart; the K step of 16
+// elements advances the start address by 32 bytes inside the atom). Thread 0 waits for
+// a stage's copies (mbarrier complete_tx), issues its four MMAs, commits them to the
+// stage's "empty" barrier, and refills the previous stage once its MMAs are done, so
+// the tensor pipe always has queued work. 96 KB of stages: two CTAs per SM, one's
+// epilogue overlapping the other's main loop. Bounded waits as above.
 namespace tma {
-constexpr int S = 4, BK = 32;
+constexpr int S = 2, BK = 64;
 constexpr int A_ST = tc::BM * BK * 2, B_ST = tc::BN * BK * 2, STAGE = A_ST + B_ST;
-constexpr int LBO_A = tc::BM * 16, LBO_B = tc::BN * 16;  // bytes between K chunks
-constexpr int SMEM = S * STAGE + 1024 + 128;             // + alignment slack + barriers
+constexpr int SMEM = S * STAGE + 1024 + 128;  // + alignment slack + barriers
 }  // namespace tma
+
+// K-major SWIZZLE_128B operand descriptor: start address, leading offset unused (1),
+// stride 1024 bytes between 8-row atoms, sm_100 version bits, layout type 2.
+__device__ __forceinline__ uint64_t tc_sdesc_sw128(uint32_t saddr) {
+  uint64_t d = (uint64_t)((saddr >> 4) & 0x3FFFu);
+  d |= (uint64_t)1 << 16;
+  d |= (uint64_t)(1024 >> 4) << 32;
+  d |= (uint64_t)1 << 46;
+  d |= (uint64_t)2 << 61;
+  return d;
+}
 
 __device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap* map, int x, int y, uint32_t mbar) {
   asm volatile(
@@ -501,11 +513,8 @@ __global__ void __launch_bounds__(tc::THREADS) gemm_tma_kernel(const __grid_cons
       const int s = t % tma::S, k0 = (kt0 + t) * tma::BK;
       const uint32_t st = sbase + s * tma::STAGE, fb = full0 + 8 * s;
       asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(fb), "r"(tma::STAGE) : "memory");
-#pragma unroll
-      for (int j = 0; j < tma::BK / 8; ++j) {
-        tma_load_2d(st + j * tma::LBO_A, &tmA, k0 + 8 * j, m0, fb);
-        tma_load_2d(st + tma::A_ST + j * tma::LBO_B, &tmB, k0 + 8 * j, n0, fb);
-      }
+      tma_load_2d(st, &tmA, k0, m0, fb);
+      tma_load_2d(st + tma::A_ST, &tmB, k0, n0, fb);
     };
     int issued = 0, consumed = 0;
     for (; issued < min(tma::S, nt); ++issued) issue(issued);
@@ -520,8 +529,8 @@ __global__ void __launch_bounds__(tc::THREADS) gemm_tma_kernel(const __grid_cons
       const uint32_t a0 = sbase + s * tma::STAGE, b0 = a0 + tma::A_ST;
 #pragma unroll
       for (int kk = 0; kk < tma::BK / 16; ++kk) {
-        const uint64_t da = tc_sdesc(a0 + kk * 2 * tma::LBO_A, tma::LBO_A, 128);
-        const uint64_t db = tc_sdesc(b0 + kk * 2 * tma::LBO_B, tma::LBO_B, 128);
+        const uint64_t da = tc_sdesc_sw128(a0 + kk * 32);
+        const uint64_t db = tc_sdesc_sw128(b0 + kk * 32);
         const uint32_t acc = (it > 0 || kk > 0) ? 1u : 0u;
         asm volatile(
             "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
@@ -552,6 +561,9 @@ __global__ void __launch_bounds__(tc::THREADS) gemm_tma_kernel(const __grid_cons
   if (!ok && tid == 0) atomicExch(&g_tc_error, 1);
   asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
   const int m = m0 + warp * 32 + lane;
+  // plain f32 output (no epilogue terms): two 16-byte stores per 8 columns
+  const bool plain = p.outf && !p.atomic && !p.outh && !p.cadd && !p.bias_m && !p.bias_n && !p.pre && p.act == 0 &&
+                     (p.ldc & 3) == 0 && ((reinterpret_cast<uintptr_t>(p.outf) & 15u) == 0u);
   if (ok) {
     for (int c0 = 0; c0 < tc::BN; c0 += 8) {
       uint32_t v[8];
@@ -565,21 +577,29 @@ __global__ void __launch_bounds__(tc::THREADS) gemm_tma_kernel(const __grid_cons
 #pragma unroll
         for (int e = 0; e < 8; ++e) v[e] = 0u;
       }
+      if (plain && m < p.M && n0 + c0 + 8 <= p.N) {
+        float4* q = reinterpret_cast<float4*>(p.outf + (long long)m * p.ldc + n0 + c0);
+        q[0] = make_float4(p.alpha * __uint_as_float(v[0]), p.alpha * __uint_as_float(v[1]),
+                           p.alpha * __uint_as_float(v[2]), p.alpha * __uint_as_float(v[3]));
+        q[1] = make_float4(p.alpha * __uint_as_float(v[4]), p.alpha * __uint_as_float(v[5]),
+                           p.alpha * __uint_as_float(v[6]), p.alpha * __uint_as_float(v[7]));
+      } else {
 #pragma unroll
-      for (int e = 0; e < 8; ++e) {
-        const int n = n0 + c0 + e;
-        if (m >= p.M || n >= p.N) continue;
-        float x = p.alpha * __uint_as_float(v[e]);
-        if (p.cadd) x += p.cadd[(long long)m * p.ldadd + n];
-        if (p.bias_m) x += p.bias_m[m];
-        if (p.bias_n) x += p.bias_n[n];
-        if (p.pre) p.pre[(long long)m * p.ldpre + n] = __float2bfloat16_rn(x);
-        if (p.act == 1) x = gelu_f(x);
-        const long long o = (long long)m * p.ldc + n;
-        if (p.outf) {
-          if (p.atomic) atomicAdd(p.outf + o, x); else p.outf[o] = x;
+        for (int e = 0; e < 8; ++e) {
+          const int n = n0 + c0 + e;
+          if (m >= p.M || n >= p.N) continue;
+          float x = p.alpha * __uint_as_float(v[e]);
+          if (p.cadd) x += p.cadd[(long long)m * p.ldadd + n];
+          if (p.bias_m) x += p.bias_m[m];
+          if (p.bias_n) x += p.bias_n[n];
+          if (p.pre) p.pre[(long long)m * p.ldpre + n] = __float2bfloat16_rn(x);
+          if (p.act == 1) x = gelu_f(x);
+          const long long o = (long long)m * p.ldc + n;
+          if (p.outf) {
+            if (p.atomic) atomicAdd(p.outf + o, x); else p.outf[o] = x;
+          }
+          if (p.outh) p.outh[o] = __float2bfloat16_rn(x);
         }
-        if (p.outh) p.outh[o] = __float2bfloat16_rn(x);
       }
     }
   }
@@ -606,16 +626,17 @@ EncodeTiledFn encode_fn() {
 }
 
 // 2D map over a row-major bf16 matrix of `rows` x `cols` (cols contiguous, ld elements
-// per row), box 8 columns x box_rows rows; out-of-range elements read as zero.
+// per row), box 64 columns (128 bytes, the swizzle span) x box_rows rows, 128-byte
+// swizzle; out-of-range elements read as zero.
 bool make_map(CUtensorMap* map, const bf16* base, long long rows, long long cols, long long ld, int box_rows) {
   EncodeTiledFn fn = encode_fn();
   if (!fn) return false;
   const cuuint64_t dim[2] = {(cuuint64_t)cols, (cuuint64_t)rows};
   const cuuint64_t stride[1] = {(cuuint64_t)ld * 2};
-  const cuuint32_t box[2] = {8u, (cuuint32_t)box_rows};
+  const cuuint32_t box[2] = {(cuuint32_t)tma::BK, (cuuint32_t)box_rows};
   const cuuint32_t estride[2] = {1u, 1u};
   return fn(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<bf16*>(base), dim, stride, box, estride,
-            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
