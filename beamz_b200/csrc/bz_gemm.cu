@@ -203,27 +203,61 @@ __global__ void __launch_bounds__(32 * WM * WN) gemm_bf16_kernel(GemmP p) {
     }
   }
 
-  // epilogue
+  // epilogue: each thread holds pairs of adjacent columns (e, e+1); pairs go through
+  // 8-byte f32 and 4-byte bf16x2 accesses when both columns exist and the row offsets
+  // are even, single elements otherwise
+  const bool even = ((p.ldc | p.sc | p.ldadd | p.sadd | p.ldpre | p.spre) & 1) == 0 &&
+                    ((reinterpret_cast<uintptr_t>(p.cadd) | reinterpret_cast<uintptr_t>(p.outf)) & 7u) == 0 &&
+                    ((reinterpret_cast<uintptr_t>(p.outh) | reinterpret_cast<uintptr_t>(p.pre)) & 3u) == 0;
 #pragma unroll
   for (int i = 0; i < MT; ++i)
 #pragma unroll
     for (int j = 0; j < NT; ++j)
 #pragma unroll
-      for (int e = 0; e < 4; ++e) {
-        const int m = m0 + wm0 + i * 16 + (lane >> 2) + (e >= 2 ? 8 : 0);
-        const int n = n0 + wn0 + j * 8 + (lane & 3) * 2 + (e & 1);
+      for (int h = 0; h < 2; ++h) {
+        const int m = m0 + wm0 + i * 16 + (lane >> 2) + h * 8;
+        const int n = n0 + wn0 + j * 8 + (lane & 3) * 2;
         if (m >= p.M || n >= p.N) continue;
-        float v = p.alpha * acc[i][j][e];
-        if (p.cadd) v += p.cadd[(long long)bz * p.sadd + (long long)m * p.ldadd + n];
-        if (p.bias_m) v += p.bias_m[m];
-        if (p.bias_n) v += p.bias_n[n];
-        if (p.pre) p.pre[(long long)bz * p.spre + (long long)m * p.ldpre + n] = __float2bfloat16_rn(v);
-        if (p.act == 1) v = gelu_f(v);
+        float v[2] = {p.alpha * acc[i][j][2 * h], p.alpha * acc[i][j][2 * h + 1]};
+        const bool pair = even && n + 1 < p.N && !p.atomic;
+        const int cnt = n + 1 < p.N ? 2 : 1;
+        if (p.cadd) {
+          const float* q = p.cadd + (long long)bz * p.sadd + (long long)m * p.ldadd + n;
+          if (pair) {
+            const float2 a = *reinterpret_cast<const float2*>(q);
+            v[0] += a.x;
+            v[1] += a.y;
+          } else {
+            for (int e = 0; e < cnt; ++e) v[e] += q[e];
+          }
+        }
+        for (int e = 0; e < cnt; ++e) {
+          if (p.bias_m) v[e] += p.bias_m[m];
+          if (p.bias_n) v[e] += p.bias_n[n + e];
+        }
+        if (p.pre) {
+          bf16* q = p.pre + (long long)bz * p.spre + (long long)m * p.ldpre + n;
+          if (pair) *reinterpret_cast<__nv_bfloat162*>(q) = __floats2bfloat162_rn(v[0], v[1]);
+          else for (int e = 0; e < cnt; ++e) q[e] = __float2bfloat16_rn(v[e]);
+        }
+        if (p.act == 1) {
+          v[0] = gelu_f(v[0]);
+          v[1] = gelu_f(v[1]);
+        }
         const long long o = (long long)bz * p.sc + (long long)m * p.ldc + n;
         if (p.outf) {
-          if (p.atomic) atomicAdd(p.outf + o, v); else p.outf[o] = v;
+          if (p.atomic) {
+            for (int e = 0; e < cnt; ++e) atomicAdd(p.outf + o + e, v[e]);
+          } else if (pair) {
+            *reinterpret_cast<float2*>(p.outf + o) = make_float2(v[0], v[1]);
+          } else {
+            for (int e = 0; e < cnt; ++e) p.outf[o + e] = v[e];
+          }
         }
-        if (p.outh) p.outh[o] = __float2bfloat16_rn(v);
+        if (p.outh) {
+          if (pair) *reinterpret_cast<__nv_bfloat162*>(p.outh + o) = __floats2bfloat162_rn(v[0], v[1]);
+          else for (int e = 0; e < cnt; ++e) p.outh[o + e] = __float2bfloat16_rn(v[e]);
+        }
       }
 }
 
