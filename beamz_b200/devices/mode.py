@@ -28,8 +28,8 @@ from ..const import LIGHT_SPEED
 
 
 def compute_derivative_matrices(N, dL, npml=0):
-    fwd = sps.diags([-1, 1], [0, 1], shape=(N, N), format="csr") / dL
-    bwd = sps.diags([-1, 1], [-1, 0], shape=(N, N), format="csr") / dL
+    fwd = sps.diags([-1.0, 1.0], [0, 1], shape=(N, N), format="csr", dtype=float) / dL
+    bwd = sps.diags([-1.0, 1.0], [-1, 0], shape=(N, N), format="csr", dtype=float) / dL
     if npml > 1:
         stretch = np.ones(N, dtype=complex)
         strength, power = 3.0, 3

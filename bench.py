@@ -68,6 +68,18 @@ def workload(name, n_steps=None):
     return d, t, dx, desc
 
 
+def max_over_ranks(ms: float, world: int, device="cpu") -> float:
+    """The slowest rank's time (every rank takes part; a no-op for one rank)."""
+    if world <= 1:
+        return ms
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([ms], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 # ---------------------------------------------------------------------------- clocks
 class ClockSampler:
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
@@ -212,10 +224,7 @@ def run_b200(args):
     ck = clocks.stop()
     total_ms = t_start.elapsed_time(t_end)
     run_ms = [a.elapsed_time(b) for a, b in evs]
-    if world > 1:
-        tt = torch.tensor([total_ms], device="cuda")
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        total_ms = float(tt.item())
+    total_ms = max_over_ranks(total_ms, world, "cuda")
     value = world * args.steps * cells * n_steps / (total_ms * 1e-3) / 1e9
 
     # dominant kernel: the time-blocked step launch (time_block steps per launch); the
