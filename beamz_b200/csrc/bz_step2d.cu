@@ -358,6 +358,20 @@ __global__ void __launch_bounds__(32 * NW) step2d_tb_kernel(
   bool own[2];
   own[0] = lane >= TS && xs[0] < nx;
   own[1] = lane < 32 - TS && xs[1] < nx;
+  // owned cells inside the capture box (adjoint recompute): bit i*2+j
+  unsigned cap = 0u;
+  if (o.region != nullptr) {
+#pragma unroll
+    for (int i = 0; i < R; ++i) {
+      const int tr = w * R + i, y = yb + i;
+#pragma unroll
+      for (int j = 0; j < 2; ++j) {
+        const int rx = xs[j] - o.rx0, ry = y - o.ry0;
+        if (own[j] && tr >= TS && tr < TH - TS && y < ny && rx >= 0 && rx < o.rw && ry >= 0 && ry < o.rh)
+          cap |= 1u << (i * 2 + j);
+      }
+    }
+  }
 
 #pragma unroll 1
   for (int s = 0; s < TS; ++s) {
@@ -443,6 +457,22 @@ __global__ void __launch_bounds__(32 * NW) step2d_tb_kernel(
               if (xo == xs[j]) ez[i][j][k] = fma_rn(m, ez[i][j][k], mul_rn(wv, sv));
           }
         }
+      }
+    }
+    // Ez after this sub-step inside the capture box (the box holds no sources)
+    if (cap) {
+      const long long slot = step + 1 - o.reg_step0;
+      if (slot >= 1 && slot < o.n_reg) {
+#pragma unroll
+        for (int i = 0; i < R; ++i)
+#pragma unroll
+          for (int j = 0; j < 2; ++j)
+            if (cap & (1u << (i * 2 + j))) {
+              const int rx = xs[j] - o.rx0, ry = yb + i - o.ry0;
+#pragma unroll
+              for (int k = 0; k < NC; ++k)
+                o.region[(((slot * g.n_designs + d) * NC + k) * o.rh + ry) * (long long)o.rw + rx] = ez[i][j][k];
+            }
       }
     }
     // Monitor samples of owned cells: record and DFT ring
@@ -562,7 +592,16 @@ int launch_tb(const bz_grid2d* gd, const bz_fields2d* f, const bz_source_ops* s,
               int64_t step, const int64_t* d_step, cudaStream_t st) {
   constexpr int OW = 64 - 2 * TS, OH = NW * R - 2 * TS;
   const Geo2D<T> g = make_geo<T>(gd);
-  const Ops2D<T> o = make_ops<T>(s, m);
+  Ops2D<T> o = make_ops<T>(s, m);
+  if (m && m->region && m->n_reg > 1) {
+    o.region = (T*)m->region;
+    o.rx0 = m->rx0;
+    o.ry0 = m->ry0;
+    o.rw = m->rw;
+    o.rh = m->rh;
+    o.n_reg = m->n_reg;
+    o.reg_step0 = m->reg_step0;
+  }
   const int src = (int)(step & 1);
   dim3 grid((unsigned)ceil_div(gd->nx, OW), (unsigned)ceil_div(gd->ny, OH), (unsigned)gd->n_designs);
   step2d_tb_kernel<T, NC, TS, R, NW><<<grid, 32 * NW, 0, st>>>(
@@ -696,8 +735,8 @@ extern "C" int bz_step2d_multi(const bz_grid2d* g, const bz_fields2d* f, const b
              n_sub);
   BZ_REQUIRE(tile >= 0 && tile <= 5, "bz_step2d_multi: tile must be 0..5 (got %d)", tile);
   if (n_sub == 1) return bz_step2d(g, f, s, m, step, d_step, stream);
-  if (f->power != nullptr || (m && m->region != nullptr))
-    return bz::fail(BZ_ERR_UNSUPPORTED, "bz_step2d_multi: power accumulation and region capture need bz_step2d");
+  if (f->power != nullptr)
+    return bz::fail(BZ_ERR_UNSUPPORTED, "bz_step2d_multi: power accumulation needs bz_step2d");
   cudaStream_t st = bz::as_stream(stream);
   if (g->dtype == BZ_F32)
     return g->n_comp == 1 ? bz::tb_by_steps<float, 1>(g, f, s, m, step, n_sub, tile, d_step, st)

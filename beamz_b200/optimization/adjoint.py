@@ -219,8 +219,7 @@ class AdjointFDTD2D:
             cap[0].copy_(self.ckpt[s][0][:, 0, y0:y0 + h, x0:x0 + w])
             mo.ring, mo.region, mo.n_reg = None, cap.data_ptr(), s1 - s0 + 1
             mo.rx0, mo.ry0, mo.rw, mo.rh, mo.reg_step0 = x0, y0, w, h, s0
-            for n in range(s0, s1):
-                eng._launch(n, None)
+            eng.advance_direct(s1 - s0)
             st_.fwd_step0, st_.n_fwd = s0, s1 - s0 + 1
             for n in range(s1 - 1, s0 - 1, -1):
                 nat.adjoint_step2d(grid, st_, ops, n, phase, st)

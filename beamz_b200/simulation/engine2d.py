@@ -212,8 +212,19 @@ class Engine2D:
                          d_step_ptr, self._stream())
 
     def _block(self) -> int:
-        """Steps per launch available now (the capture box needs single steps)."""
-        return 1 if self.mops.region else self.time_block
+        """Steps per launch available now."""
+        return self.time_block
+
+    def advance_direct(self, n: int):
+        """Advance n steps with direct launches (blocked where possible, no graphs): for
+        runs whose launch parameters change between calls, such as the adjoint's
+        segment recompute with region capture."""
+        while n > 0:
+            tb = self.time_block if n >= self.time_block else 1
+            (self._launch_tb if tb > 1 else self._launch)(self.step_index, None)
+            self.n_step_launches += 1
+            self.step_index += tb
+            n -= tb
 
     def step_once(self):
         """Advance one time step with a direct launch."""
@@ -309,7 +320,7 @@ class Engine2D:
             if self.record is not None:
                 room = min(room, self.mops.rec_step0 + self.rec_rows - self.step_index)
             tb = self._block()
-            if self.use_graphs and tb == self.time_block and room >= self.chunk:
+            if self.use_graphs and not self.mops.region and room >= self.chunk:
                 # the chunk writes `chunk` ring slots: fold what earlier launches left
                 # there first, or those samples are overwritten before they are read
                 if self.step_index - self._folded > RING_LEN - self.chunk:

@@ -155,8 +155,8 @@ int bz_step2d(const bz_grid2d* g, const bz_fields2d* f, const bz_source_ops* src
  * n_sub: 1, 3, 5 or 7 (odd, so the copy read stays (step & 1) and the result lands
  * in copy ((step + n_sub) & 1)); 1 is bz_step2d. tile: 0 = default (4x16), 1..5 =
  * tile shapes of 4x8, 4x16, 8x8, 5x16 and 6x12 (rows per warp x warps) for float32
- * single-component fields. Power accumulation and region capture return BZ_ERR_UNSUPPORTED (use
- * bz_step2d for those steps). */
+ * single-component fields. Region capture (mon->region) is taken per sub-step; power
+ * accumulation returns BZ_ERR_UNSUPPORTED (use bz_step2d for those steps). */
 int bz_step2d_multi(const bz_grid2d* g, const bz_fields2d* f, const bz_source_ops* src,
                     const bz_monitor_ops* mon, int64_t step, int32_t n_sub, int32_t tile,
                     const int64_t* d_step, void* stream);
