@@ -129,6 +129,8 @@ _raster3d = _sig("bz_rasterize3d", C.c_int, [i32, i32, i32, i32, vp, vp, vp, vp,
                                               vp, f64, f64, f64, f64, vp, vp, vp, vp])
 _adjoint2d = _sig("bz_adjoint_step2d", C.c_int, [C.POINTER(Grid2D), C.POINTER(Adjoint2D), C.POINTER(SourceOps), i64,
                                                   i32, vp])
+_adjoint2d_multi = _sig("bz_adjoint_step2d_multi", C.c_int, [C.POINTER(Grid2D), C.POINTER(Adjoint2D),
+                                                              C.POINTER(SourceOps), i64, i32, i32, vp])
 _advance = _sig("bz_advance_step", C.c_int, [vp, i64, vp])
 _prepare = _sig("bz_prepare_coeffs", C.c_int, [vp, vp, i64, i32, i32, i32, f64, f64, f64, vp, vp, vp])
 _upd_h2d = _sig("bz_update_h2d", C.c_int, [i32, i32, i32, i32, vp, vp, vp, vp, f64, f64, f64, f64, f64, vp])
@@ -149,7 +151,7 @@ _gemm_err = _sig("bz_gemm_error", C.c_int, [C.POINTER(i32), i32])
 
 #: every symbol include/beamz_b200.h declares (checked by the CPU test suite)
 EXPORTED = ["bz_version", "bz_last_error", "bz_step2d", "bz_step2d_multi", "bz_dft_fold", "bz_step2d_dft_static", "bz_advance_step",
-            "bz_adjoint_step2d", "bz_step3d", "bz_cell_ops", "bz_gather", "bz_power3d", "bz_dft_fold_q", "bz_rasterize3d", "bz_prepare_coeffs", "bz_update_h2d",
+            "bz_adjoint_step2d", "bz_adjoint_step2d_multi", "bz_step3d", "bz_cell_ops", "bz_gather", "bz_power3d", "bz_dft_fold_q", "bz_rasterize3d", "bz_prepare_coeffs", "bz_update_h2d",
             "bz_update_e2d", "bz_rasterize2d", "bz_gemm_bf16", "bz_spectral_mix", "bz_spectral_mix_bwd", "bz_gelu_bwd",
             "bz_row_mean", "bz_row_broadcast", "bz_chan_sum", "bz_adam", "bz_to_bf16", "bz_gemm_error"]
 
@@ -236,6 +238,11 @@ def rasterize3d(*args) -> None:
 
 def adjoint_step2d(grid, state, ops, step, phase, stream) -> None:
     check(_adjoint2d(C.byref(grid), C.byref(state), C.byref(ops) if ops is not None else None, step, phase, stream))
+
+
+def adjoint_step2d_multi(grid, state, ops, step: int, n_sub: int, phase: int, stream: int) -> None:
+    check(_adjoint2d_multi(C.byref(grid), C.byref(state), C.byref(ops) if ops is not None else None, step, n_sub,
+                           phase, stream))
 
 
 # ---- surrogate kernels -------------------------------------------------------------

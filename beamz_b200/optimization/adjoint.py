@@ -84,6 +84,7 @@ class AdjointFDTD2D:
                 raise ValueError("sources may not act inside the design region")
         self._fwd_ops = src_ops
         self.engine = None
+        self._adj_block = None  # reverse steps per launch, timed on the first backward
 
     # ---- helpers -------------------------------------------------------------
     def _eps_full(self, eps_region):
@@ -208,6 +209,8 @@ class AdjointFDTD2D:
             st_.e[i], st_.hx[i], st_.hy[i] = E[i].data_ptr(), HX[i].data_ptr(), HY[i].data_ptr()
         phase = 0
         grid = eng.grid
+        if self._adj_block is None:
+            self._adj_block = self._time_adjoint(grid, st_, st)
         mo = eng.mops
         saved = (mo.ring, mo.region, mo.n_reg)
         for s in range(len(self.ckpt) - 1, -1, -1):
@@ -221,13 +224,42 @@ class AdjointFDTD2D:
             mo.rx0, mo.ry0, mo.rw, mo.rh, mo.reg_step0 = x0, y0, w, h, s0
             eng.advance_direct(s1 - s0)
             st_.fwd_step0, st_.n_fwd = s0, s1 - s0 + 1
-            for n in range(s1 - 1, s0 - 1, -1):
-                nat.adjoint_step2d(grid, st_, ops, n, phase, st)
+            n, tb = s1 - 1, self._adj_block
+            while n >= s0:  # blocks of tb reverse steps, single steps for the rest
+                k = tb if n - s0 + 1 >= tb else 1
+                nat.adjoint_step2d_multi(grid, st_, ops, n, k, phase, st)
                 phase ^= 1
+                n -= k
         mo.ring, mo.region, mo.n_reg = saved
         eng._graphs.clear()
         torch.cuda.current_stream().synchronize()
         return grad.cpu().numpy() / self._adj_scale[:, None, None]
+
+    def _time_adjoint(self, grid, state, stream, reps: int = 3) -> int:
+        """Blocked or single reverse steps, whichever runs faster on this problem (a
+        single design on a small grid leaves the blocked tiles too few to fill the GPU).
+        Timed before the backward pass: no gradient, no operations, and every launch reads
+        the still-zero current copy, so nothing changes."""
+        tb = self.engine.time_block
+        if tb <= 1:
+            return 1
+        grad = state.grad
+        state.grad = None
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        best = {}
+        for k in (tb, 1):
+            nat.adjoint_step2d_multi(grid, state, None, tb - 1, k, 0, stream)  # warm-up
+            t = float("inf")
+            for _ in range(reps):
+                a.record()
+                for _ in range(tb // k):
+                    nat.adjoint_step2d_multi(grid, state, None, tb - 1, k, 0, stream)
+                b.record()
+                b.synchronize()
+                t = min(t, a.elapsed_time(b))
+            best[k] = t
+        state.grad = grad
+        return min(best, key=best.get)
 
     def value_and_grad(self, eps_region):
         J = self.forward(eps_region)

@@ -218,6 +218,14 @@ typedef struct bz_adjoint2d {
 int bz_adjoint_step2d(const bz_grid2d* g, const bz_adjoint2d* s, const bz_source_ops* ops, int64_t step,
                       int32_t phase, void* stream);
 
+/* n_sub reverse steps of bz_adjoint_step2d in one launch (step, step-1, ...,
+ * step-n_sub+1; temporal blocking with the register tile of bz_step2d_multi): the same
+ * gradient and operations per reverse step. n_sub: 1, 3, 5 or 7 (odd, so the copy read
+ * is (phase & 1) and the result lands in the other copy, as n_sub single calls with
+ * alternating phase leave it); step + 1 >= n_sub. */
+int bz_adjoint_step2d_multi(const bz_grid2d* g, const bz_adjoint2d* s, const bz_source_ops* ops, int64_t step,
+                            int32_t n_sub, int32_t phase, void* stream);
+
 /* Adds n to the device step counter (*d_step += n). */
 int bz_advance_step(int64_t* d_step, int64_t n, void* stream);
 

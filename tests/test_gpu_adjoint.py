@@ -149,3 +149,26 @@ def test_multifrequency_weighted_objective_matches_central_differences(bz):
         em[0, i, j] -= h
         fd = (multi.forward(ep, keep_checkpoints=False)[0] - multi.forward(em, keep_checkpoints=False)[0]) / (2 * h)
         assert abs(fd - g[0, i, j]) <= 1e-5 * max(abs(fd), 1e-3 * np.abs(g).max()), (i, j, fd, g[0, i, j])
+
+
+@pytest.mark.parametrize("K", [128, 100])
+def test_blocked_adjoint_matches_single_steps(bz, K):
+    """Reverse steps taken in blocks (bz_adjoint_step2d_multi) against single reverse
+    steps: same objective, gradient within 1e-12 (float64)."""
+    from beamz_b200.optimization.adjoint import AdjointFDTD2D
+
+    prob, er, eps, sigma, dx, dt, n_steps, src, mon, mode, f0, region = _problem(bz, B=2, K=K, seed=4)
+    freqs = [0.97 * f0, f0]
+    grads = []
+    for single in (False, True):
+        p = AdjointFDTD2D(eps, sigma, dx, dt, n_steps, [src], mon, np.stack([mode, mode]), freqs, region,
+                          n_designs=2, precision="fp64", checkpoint_every=K)
+        J = p.forward(er)
+        if single:
+            p.engine.time_block, p.engine._autotune = 1, False
+        else:
+            assert p.engine.time_block > 1
+        grads.append((J, p.backward()))
+    np.testing.assert_allclose(grads[0][0], grads[1][0], rtol=1e-12)
+    g0, g1 = grads[0][1], grads[1][1]
+    assert np.linalg.norm(g0 - g1) <= 1e-12 * np.linalg.norm(g1)
