@@ -73,7 +73,7 @@ class Gemm(C.Structure):
 
 class Grid3D(C.Structure):
     _fields_ = [("nx", i32), ("ny", i32), ("nz", i32), ("pitch", i32), ("n_designs", i32), ("n_comp", i32),
-                ("n_mat", i32), ("dtype", i32), ("tile_z", i32), ("reserved", i32), ("chx", f64), ("chy", f64),
+                ("n_mat", i32), ("dtype", i32), ("tile_z", i32), ("tile_y", i32), ("chx", f64), ("chy", f64),
                 ("chz", f64), ("qx", f64), ("qz", f64), ("inv_kd2", f64)]
 
 

@@ -20,7 +20,7 @@ namespace bz {
 namespace {
 
 constexpr unsigned FULL = 0xffffffffu;
-constexpr int TX = 32, TY = 8;
+constexpr int TX = 32;  // tile width; the tile height TY is a template parameter (8 or 16)
 
 template <typename T>
 struct Geo3D {
@@ -70,7 +70,7 @@ struct PlaneIn {
   T a, ce;
 };
 
-template <typename T, int NC, int ZB>
+template <typename T, int NC, int ZB, int TY>
 __global__ void __launch_bounds__(TX * TY) step3d_kernel(Ptr3<T> in, Out3<T> out, const T* __restrict__ ce,
                                                           const T* __restrict__ loss, Geo3D<T> g) {
   __shared__ T s_ez[NC][TY][TX], s_ex[NC][TY][TX], s_hz[NC][TY][TX], s_hx[NC][TY][TX];
@@ -219,7 +219,7 @@ __global__ void __launch_bounds__(TX * TY) step3d_kernel(Ptr3<T> in, Out3<T> out
   }
 }
 
-template <typename T, int NC, int ZB>
+template <typename T, int NC, int ZB, int TY>
 int launch3d(const bz_grid3d* gd, const bz_fields3d* f, int64_t step, cudaStream_t st) {
   Geo3D<T> g;
   g.nx = gd->nx;
@@ -248,15 +248,20 @@ int launch3d(const bz_grid3d* gd, const bz_fields3d* f, int64_t step, cudaStream
   }
   dim3 block(TX, TY);
   dim3 grid((unsigned)ceil_div(gd->nx, TX - 1), (unsigned)ceil_div(gd->ny, TY - 1), (unsigned)(g.nzb * gd->n_designs));
-  step3d_kernel<T, NC, ZB><<<grid, block, 0, st>>>(in, out, (const T*)f->ce, (const T*)f->loss, g);
+  step3d_kernel<T, NC, ZB, TY><<<grid, block, 0, st>>>(in, out, (const T*)f->ce, (const T*)f->loss, g);
   return check_launch("bz_step3d");
+}
+
+template <typename T, int TY>
+int dispatch3d_ty(const bz_grid3d* g, const bz_fields3d* f, int64_t step, cudaStream_t st) {
+  const bool z8 = g->tile_z == 8;
+  if (g->n_comp == 1) return z8 ? launch3d<T, 1, 8, TY>(g, f, step, st) : launch3d<T, 1, 16, TY>(g, f, step, st);
+  return z8 ? launch3d<T, 2, 8, TY>(g, f, step, st) : launch3d<T, 2, 16, TY>(g, f, step, st);
 }
 
 template <typename T>
 int dispatch3d(const bz_grid3d* g, const bz_fields3d* f, int64_t step, cudaStream_t st) {
-  const bool z8 = g->tile_z == 8;
-  if (g->n_comp == 1) return z8 ? launch3d<T, 1, 8>(g, f, step, st) : launch3d<T, 1, 16>(g, f, step, st);
-  return z8 ? launch3d<T, 2, 8>(g, f, step, st) : launch3d<T, 2, 16>(g, f, step, st);
+  return g->tile_y == 16 ? dispatch3d_ty<T, 16>(g, f, step, st) : dispatch3d_ty<T, 8>(g, f, step, st);
 }
 
 // ---------------------------------------------------------------------------- cell ops
@@ -345,6 +350,7 @@ extern "C" int bz_step3d(const bz_grid3d* g, const bz_fields3d* f, int64_t step,
   BZ_REQUIRE(g->n_designs >= 1 && g->n_designs * bz::ceil_div(g->nz, 8) <= 65535, "bz_step3d: too many designs");
   BZ_REQUIRE(g->n_mat == 1 || g->n_mat == g->n_designs, "bz_step3d: n_mat must be 1 or n_designs");
   BZ_REQUIRE(g->tile_z == 0 || g->tile_z == 8 || g->tile_z == 16, "bz_step3d: tile_z must be 0, 8 or 16");
+  BZ_REQUIRE(g->tile_y == 0 || g->tile_y == 8 || g->tile_y == 16, "bz_step3d: tile_y must be 0, 8 or 16");
   for (int c = 0; c < 2; ++c)
     for (int i = 0; i < 3; ++i) BZ_REQUIRE(f->e[c][i] && f->h[c][i], "bz_step3d: field buffer is NULL");
   BZ_REQUIRE(f->ce && f->loss, "bz_step3d: coefficient arrays are NULL");

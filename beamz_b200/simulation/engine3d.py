@@ -28,7 +28,7 @@ def _round_up(n, m):
 
 class Engine3D:
     def __init__(self, eps_r, sigma, dx, dy, dz, dt, n_steps, sources, monitors, *, precision="fp32", n_comp=None,
-                 power=False, n_designs=1, record=True, use_graphs=True, tile_z=16, device=None):
+                 power=False, n_designs=1, record=True, use_graphs=True, tile_z=16, tile_y=8, device=None):
         if not torch.cuda.is_available():
             raise RuntimeError("beamz_b200 needs a CUDA GPU (sm_100a); none is visible")
         self.dev = torch.device("cuda", torch.cuda.current_device()) if device is None else torch.device(device)
@@ -67,6 +67,7 @@ class Engine3D:
         g = nat.Grid3D()
         g.nx, g.ny, g.nz, g.pitch = self.nx, self.ny, self.nz, self.pitch
         g.n_designs, g.n_comp, g.n_mat, g.dtype, g.tile_z = n_designs, self.n_comp, self.n_mat, self.bz_dtype, tile_z
+        g.tile_y = int(tile_y)
         g.chx, g.chy, g.chz = self.dt / (MU_0 * self.dx), self.dt / (MU_0 * self.dy), self.dt / (MU_0 * self.dz)
         g.qx, g.qz = self.dy / self.dx, self.dy / self.dz
         g.inv_kd2 = 2.0 * EPS_0 * self.dy / self.dt

@@ -112,7 +112,8 @@ class FDTD:
 
             self.engine = Engine3D(self.mesh.permittivity, self.mesh.conductivity, self.dx, self.dy, self.dz,
                                    self.dt, self.num_steps, self.sources, self.monitors, precision=precision,
-                                   n_comp=n_comp, power=accumulate_power, use_graphs=graphs)
+                                   n_comp=n_comp, power=accumulate_power, use_graphs=graphs,
+                                   tile_z=opts.get("tile_z", 16), tile_y=opts.get("tile_y", 8))
         else:
             from .engine2d import Engine2D
 

@@ -264,7 +264,7 @@ typedef struct bz_grid3d {
   int32_t nx, ny, nz, pitch;
   int32_t n_designs, n_comp, n_mat, dtype;
   int32_t tile_z;           /* z planes per thread block: 8 or 16 (0 = 16) */
-  int32_t reserved;
+  int32_t tile_y;           /* rows per thread block (32 x tile_y threads): 8 or 16 (0 = 8) */
   double chx, chy, chz, qx, qz, inv_kd2;
 } bz_grid3d;
 
