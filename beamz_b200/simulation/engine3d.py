@@ -79,6 +79,11 @@ class Engine3D:
         self.d_step = torch.zeros(1, dtype=torch.int64, device=self.dev)
         self.use_graphs = use_graphs
         self._graphs = {}
+        # kernels per step: the step itself, source operations, monitor gather, power
+        self.kernels_per_step = 1 + (self.sops.n_ops > 0) + (self.gops is not None) + (self.power is not None)
+        self.n_step_launches = 0  # bz_step3d launches (one per step, graph nodes included)
+        self.n_kernel_launches = 0  # every launch of this library, folds included
+        self.n_fold_launches = 0
         torch.cuda.current_stream().synchronize()
 
     @staticmethod
@@ -191,6 +196,8 @@ class Engine3D:
     def step_once(self):
         self._maybe_drain()
         self._launch(self.step_index, None)
+        self.n_step_launches += 1
+        self.n_kernel_launches += self.kernels_per_step
         self.step_index += 1
         if self.dft is not None and self.step_index - self._folded >= RING_LEN:
             self._fold()
@@ -222,6 +229,8 @@ class Engine3D:
                 g = self._graph_for(phase)
                 self.d_step.fill_(self.step_index - phase)
                 g.replay()
+                self.n_step_launches += GRAPH_CHUNK
+                self.n_kernel_launches += GRAPH_CHUNK * self.kernels_per_step
                 self.step_index += GRAPH_CHUNK
                 n -= GRAPH_CHUNK
                 self._fold()
@@ -235,6 +244,8 @@ class Engine3D:
             nat.dft_fold_q(self.ring.data_ptr(), self.bz_dtype, RING_LEN, self.n_designs * self.n_comp * self.n_points,
                            6, 3, len(self.freqs), self.phasor.data_ptr(), self.n_steps, self._folded, cnt,
                            self.dft.data_ptr(), self._stream())
+            self.n_fold_launches += 1
+            self.n_kernel_launches += 1
             self._folded += cnt
 
     def reset(self):

@@ -36,7 +36,6 @@ sys.path.insert(0, str(ROOT))
 
 METRIC = "Gcell-updates/s (% of HBM roofline)"
 UNIT = "Gcell/s"
-BYTES_PER_CELL_2D = 32  # Ez, Hx, Hy read + write (24 B) + ce, loss (8 B), float32
 
 
 def parse():
@@ -45,7 +44,8 @@ def parse():
     p.add_argument("--steps", type=int, default=5)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    p.add_argument("--workload", default="mmi_2d", choices=["mmi_2d", "dipole_2d", "topo_2d", "surrogate_2d"])
+    p.add_argument("--workload", default="mmi_2d",
+                   choices=["mmi_2d", "dipole_2d", "soi_mmi_3d", "topo_2d", "surrogate_2d"])
     p.add_argument("--samples", type=int, default=20000, help="surrogate_2d: FDTD-labelled training samples")
     p.add_argument("--epochs", type=int, default=20, help="surrogate_2d: training epochs")
     p.add_argument("--iterations", type=int, default=15, help="surrogate_2d: plain-adjoint ascent iterations")
@@ -64,7 +64,9 @@ def workload(name, n_steps=None):
     d, t, dx = getattr(W, name)(**kw)
     desc = {"mmi_2d": "2D TE 1x2 MMI splitter, 2000x1000 cells at 20 nm, 30-cell PML, CW mode source, "
                       "5-wavelength DFT flux monitors",
-            "dipole_2d": "2D point dipole in vacuum, 400x400 cells at 20 nm, 20-cell PML, 4 edge monitors"}[name]
+            "dipole_2d": "2D point dipole in vacuum, 400x400 cells at 20 nm, 20-cell PML, 4 edge monitors",
+            "soi_mmi_3d": "3D SOI strip into a 6x3 um MMI, 600x300x150 cells at 20 nm, 16-cell PML on all faces, "
+                          "Gaussian-pulse mode source, 5-wavelength DFT flux planes on both outputs"}[name]
     return d, t, dx, desc
 
 
@@ -152,13 +154,15 @@ def profiled_traffic(kernel="step2d", workload_name="mmi_2d"):
 
 def cpu_baseline(d, t, dx, n_steps):
     """The reference's CPU loop (oracle restatement) on the first n_steps of the workload."""
-    from beamz_b200.simulation.meshing import RegularGrid  # noqa: F401 - grid from the caller
-    from oracle import fdtd2d
+    from oracle import fdtd2d, fdtd3d
 
     eps, sig = d._bench_eps, d._bench_sigma
     mons = [m for m in d.monitors]
     t0 = time.perf_counter()
-    fdtd2d.run(eps, sig, dx, dx, t[1] - t[0], n_steps, d.sources, mons, record=True)
+    if eps.ndim == 3:
+        fdtd3d.run(eps, sig, dx, dx, dx, t[1] - t[0], n_steps, d.sources, mons)
+    else:
+        fdtd2d.run(eps, sig, dx, dx, t[1] - t[0], n_steps, d.sources, mons, record=True)
     el = time.perf_counter() - t0
     cells = eps.size
     return cells * n_steps / el / 1e9, el
@@ -177,12 +181,13 @@ def run_b200(args):
         import datetime
 
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-    from beamz_b200 import FDTD, RegularGrid
+    from beamz_b200 import FDTD, RegularGrid, RegularGrid3D
 
     d, t, dx, desc = workload(args.workload, args.time_steps)
-    grid = RegularGrid(d, dx)
-    ny, nx = grid.permittivity.shape
-    cells = nx * ny
+    is3d = bool(d.is_3d and d.depth)
+    grid = RegularGrid3D(d, dx, extrude=True) if is3d else RegularGrid(d, dx)
+    shape = grid.permittivity.shape
+    cells = int(np.prod(shape))
     n_steps = len(t)
     sim = FDTD(design=grid, time=t, backend_options={"n_comp": args.n_comp})
     sim.initialize_simulation(save=False, live=False, save_memory_mode=True)
@@ -198,9 +203,10 @@ def run_b200(args):
         if evs is not None:
             evs[1].record()
 
-    l0, f0 = eng.n_step_launches, eng.n_fold_launches
+    count = (lambda: eng.n_kernel_launches) if is3d else (lambda: eng.n_step_launches + eng.n_fold_launches)
+    l0, k0 = eng.n_step_launches, count()
     one_run()
-    step_launches, fold_launches = eng.n_step_launches - l0, eng.n_fold_launches - f0
+    step_launches, all_launches = eng.n_step_launches - l0, count() - k0
 
     for _ in range(args.warmup):
         one_run()
@@ -227,14 +233,16 @@ def run_b200(args):
     total_ms = max_over_ranks(total_ms, world, "cuda")
     value = world * args.steps * cells * n_steps / (total_ms * 1e-3) / 1e9
 
-    # dominant kernel: the time-blocked step launch (time_block steps per launch); the
-    # run time also holds the DFT fold launches (<1 % by the ncu launch list)
-    tb = eng.time_block
+    # dominant kernel: the time-blocked 2D step launch (time_block steps per launch) or the
+    # 3D step launch (one step); the run time also holds the small monitor/source/fold
+    # launches (about 1 % in 2D by the ncu launch list)
+    tb = getattr(eng, "time_block", 1)
     per_launch_s = sum(run_ms) * 1e-3 / (args.steps * step_launches)
-    algo_bytes = (24 * args.n_comp + 8) * cells * n_steps / step_launches  # per launch: steps x 32 B/cell
+    cell_bytes = (48 * args.n_comp + 8) if is3d else (24 * args.n_comp + 8)
+    algo_bytes = cell_bytes * cells * n_steps / step_launches  # per launch: steps x B/cell x cells
     peak, peak_kind = measured_peaks()
     achieved = algo_bytes / per_launch_s / 1e9
-    traffic = profiled_traffic("step2d_tb", args.workload)
+    traffic = profiled_traffic("step3d" if is3d else "step2d_tb", args.workload)
 
     e2e = None
     if not args.no_e2e:
@@ -243,7 +251,7 @@ def run_b200(args):
     cpu = None
     if rank == 0 and world == 1:
         d._bench_eps, d._bench_sigma = grid.permittivity, grid.conductivity
-        ncpu = min(args.cpu_steps, n_steps)
+        ncpu = min(args.cpu_steps if not is3d else 2, n_steps)
         v, el = cpu_baseline(d, t, dx, ncpu)
         cpu = {"value": v, "unit": UNIT, "cores": 1, "kind": "port",
                "sample": f"first {ncpu} of {n_steps} time steps of the same workload, float64 NumPy "
@@ -262,22 +270,27 @@ def run_b200(args):
             "metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(total_ms / args.steps, 3), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": desc, "grid": [ny, nx], "time_steps": n_steps, "step": "one full run",
-                       "l2": "flushed (512 MB write) before every run", "parallelism": f"replicas x{world}",
-                       "time_block": tb, "tb_tile": eng.tb_tile, "tile_choice": "autotuned",
-                       "tune_us_per_step": {f"{k[0]}/{k[1]}": round(v * 1e3, 3)
-                                            for k, v in getattr(eng, "tune_times", {}).items()}},
+            "config": {"workload": desc, "grid": list(shape), "time_steps": n_steps, "step": "one full run",
+                       "l2": "flushed (512 MB write) before every run", "parallelism": f"replicas x{world}"},
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
-                         "frac": round(achieved / peak, 4), "traffic": traffic,
-                         "note": f"step2d_tb: {tb} steps per launch x {BYTES_PER_CELL_2D} B/cell (algorithmic, "
-                                 f"one-step) x {cells} cells; peak {peak_kind}; temporal blocking keeps the tile "
-                                 f"on chip between sub-steps, so DRAM traffic per launch is one read of the "
-                                 f"inputs and one write of the owned cells"},
+                         "frac": round(achieved / peak, 4), "traffic": traffic},
             "cpu_baseline": cpu,
             "e2e": {k: v for k, v in (e2e or {}).items() if not k.startswith("_")} or None,
-            "gpu_launches": args.steps * (step_launches + fold_launches),
+            "gpu_launches": args.steps * all_launches,
             "clocks": ck,
         }
+        if is3d:
+            line["config"]["tile"] = "32 x 8 columns x 16 planes"
+            line["roofline"]["note"] = (f"step3d: one step per launch x {cell_bytes} B/cell (six fields read and "
+                                        f"written, ce and loss read) x {cells} cells; peak {peak_kind}")
+        else:
+            line["config"].update(time_block=tb, tb_tile=eng.tb_tile, tile_choice="autotuned",
+                                  tune_us_per_step={f"{k[0]}/{k[1]}": round(v * 1e3, 3)
+                                                    for k, v in getattr(eng, "tune_times", {}).items()})
+            line["roofline"]["note"] = (f"step2d_tb: {tb} steps per launch x {cell_bytes} B/cell (algorithmic, "
+                                        f"one-step) x {cells} cells; peak {peak_kind}; temporal blocking keeps the "
+                                        f"tile on chip between sub-steps, so DRAM traffic per launch is one read "
+                                        f"of the inputs and one write of the owned cells")
         if flux:
             line["transmission"] = flux
         print(json.dumps(line), flush=True)
@@ -317,6 +330,10 @@ def run_reference(args):
     if rank != 0:
         return
     d, t, dx, desc = workload(args.workload, args.time_steps)
+    if d.is_3d and d.depth:
+        print(json.dumps({"impl": "reference", "unavailable": "the 3-D material grid is rasterised on the GPU "
+                          "only; the b200 line's cpu_baseline times the 3-D CPU loop on two steps"}), flush=True)
+        return
     from beamz_b200.devices.sources import GaussianSource  # noqa: F401
     from oracle import fdtd2d
 
