@@ -99,6 +99,7 @@ def compile_sources(sources, grid_shape, spacing, n_steps, is_3d=False) -> Sourc
     grid_shape is (ny, nx) or (nz, ny, nx) of the material grid; spacing is
     (dx, dy) or (dx, dy, dz). In 3D the operations act on Ez (nz-1 layers)."""
     sigs = _Signals(n_steps)
+    # events in application order, as arrays per source: cell, mul, complex weight, signal row
     ev_cell, ev_mul, ev_w, ev_sig = [], [], [], []
 
     def lin(*idx):
@@ -108,90 +109,116 @@ def compile_sources(sources, grid_shape, spacing, n_steps, is_3d=False) -> Sourc
         y, x = idx
         return y * grid_shape[1] + x
 
-    def add(cell, w, row_re, row_im):
-        ev_cell.append(cell); ev_mul.append(1.0); ev_w.append(complex(w)); ev_sig.append(row_re)  # noqa: E702
+    def emit(cells, amps, zero_cells, zero_ok, row_re, row_im):
+        """Per point i, in this order: add amps[i] on row_re at cells[i], the i*amps[i]
+        part on row_im (complex signals), then zero zero_cells[i] where zero_ok[i]."""
+        n = len(cells)
+        amps = np.asarray(amps, dtype=np.complex128)
+        parts = [(np.asarray(cells, np.int64), np.ones(n), amps, np.full(n, row_re), np.ones(n, bool))]
         if row_im is not None:  # w * (s_re + i s_im): the i*w part rides on the imaginary row
-            ev_cell.append(cell); ev_mul.append(1.0); ev_w.append(1j * complex(w)); ev_sig.append(row_im)  # noqa: E702
-
-    def zero(cell):
-        ev_cell.append(cell); ev_mul.append(0.0); ev_w.append(0j); ev_sig.append(0)  # noqa: E702
+            parts.append((np.asarray(cells, np.int64), np.ones(n), 1j * amps, np.full(n, row_im), np.ones(n, bool)))
+        if zero_cells is not None:
+            parts.append((np.asarray(zero_cells, np.int64), np.zeros(n), np.zeros(n, np.complex128), np.zeros(n, int),
+                          np.asarray(zero_ok, bool)))
+        k = len(parts)
+        cell = np.stack([q[0] for q in parts], axis=1).reshape(-1)  # point-major interleave
+        keep = np.stack([q[4] for q in parts], axis=1).reshape(-1)
+        ev_cell.append(cell[keep])
+        ev_mul.append(np.stack([q[1] for q in parts], axis=1).reshape(-1)[keep])
+        ev_w.append(np.stack([q[2] for q in parts], axis=1).reshape(-1)[keep])
+        ev_sig.append(np.stack([q[3] for q in parts], axis=1).reshape(-1)[keep].astype(np.int64))
+        del k
 
     for src in sources:
         if isinstance(src, ModeSource):
             rr, ri = sigs.add(src.signal)
             enforce = getattr(src, "enforce_direction", True)
             behind = _BEHIND.get(src.direction)
+            pts = src.mode_profiles[0]
+            if len(pts) == 0:
+                continue
+            tab = np.asarray(pts, dtype=np.complex128)  # rows (amp, x, y[, z])
+            amp, xr, yr = tab[:, 0], tab[:, 1].real, tab[:, 2].real
+            zr = tab[:, 3].real if tab.shape[1] == 4 else np.zeros(len(tab))
             if is_3d:
                 nz, ny, nx = grid_shape
                 dx, dy, dz = spacing
                 n_ez = nz - 1
+                x, y, z = np.round(xr / dx).astype(np.int64), np.round(yr / dy).astype(np.int64), \
+                    np.round(zr / dz).astype(np.int64)
+                ok = (x >= 0) & (x < nx) & (y >= 0) & (y < ny) & (z >= 0) & (z < nz)
+                x, y, z, amp = x[ok], y[ok], z[ok], amp[ok]
+                zt = np.where(z < n_ez, np.minimum(z, n_ez - 1), n_ez // 2)
+                zc = zok = None
+                if enforce and behind is not None:
+                    zz, yy, xx = zt + behind[0], y + behind[1], x + behind[2]
+                    zok = (xx >= 0) & (xx < nx) & (yy >= 0) & (yy < ny) & (zz >= 0) & (zz < n_ez)
+                    zc = lin(zz, yy, xx)
+                emit(lin(zt, y, x), amp, zc, zok, rr, ri)
             else:
                 ny, nx = grid_shape
                 dx, dy = spacing
-            for pt in src.mode_profiles[0]:
-                if len(pt) == 4:
-                    amp, xr, yr, zr = pt
-                else:
-                    amp, xr, yr = pt
-                    zr = 0
-                x, y = int(round(xr / dx)), int(round(yr / dy))
-                if is_3d:
-                    z = int(round(zr / dz))
-                    if x < 0 or x >= nx or y < 0 or y >= ny or z < 0 or z >= nz:
-                        continue
-                    zt = min(z, n_ez - 1) if z < n_ez else n_ez // 2
-                    add(lin(zt, y, x), amp, rr, ri)
-                    if enforce and behind is not None:
-                        bz_, by, bx = behind
-                        zz, yy, xx = zt + bz_, y + by, x + bx
-                        if 0 <= xx < nx and 0 <= yy < ny and 0 <= zz < n_ez:
-                            zero(lin(zz, yy, xx))
-                else:
-                    if x < 0 or x >= nx or y < 0 or y >= ny:
-                        continue
-                    add(lin(y, x), amp, rr, ri)
-                    if enforce and behind is not None and behind[0] == 0:
-                        yy, xx = y + behind[1], x + behind[2]
-                        if 0 <= xx < nx and 0 <= yy < ny:
-                            zero(lin(yy, xx))
+                x, y = np.round(xr / dx).astype(np.int64), np.round(yr / dy).astype(np.int64)
+                ok = (x >= 0) & (x < nx) & (y >= 0) & (y < ny)
+                x, y, amp = x[ok], y[ok], amp[ok]
+                zc = zok = None
+                if enforce and behind is not None and behind[0] == 0:
+                    yy, xx = y + behind[1], x + behind[2]
+                    zok = (xx >= 0) & (xx < nx) & (yy >= 0) & (yy < ny)
+                    zc = lin(yy, xx)
+                emit(lin(y, x), amp, zc, zok, rr, ri)
         elif isinstance(src, GaussianSource):
             rr, ri = sigs.add(src.signal)
             idx, amp = _gaussian_patch(src, grid_shape, spacing, is_3d)
-            cells = lin(*idx)
-            for c, a in zip(np.ravel(cells), np.ravel(amp)):
-                add(int(c), a, rr, ri)
+            emit(np.ravel(lin(*idx)), np.ravel(amp), None, None, rr, ri)
         else:
             raise TypeError(f"Unsupported source type: {type(src)}")
 
     rows = grid_shape[0] * grid_shape[1] if is_3d else grid_shape[0]
     row_len = grid_shape[2] if is_3d else grid_shape[1]
-    if not ev_cell:
+    cell = np.concatenate(ev_cell) if ev_cell else np.zeros(0, np.int64)
+    if len(cell) == 0:
         empty = np.zeros(0)
         return SourceOps(np.zeros(0, np.int32), empty, np.zeros((0, 2)), np.zeros(0, np.int32),
                          np.zeros((max(1, len(sigs.rows)), n_steps)), False, rows, np.zeros(rows + 1, np.int32))
-    cell = np.asarray(ev_cell, dtype=np.int64)
+    mul, wts, sgs = np.concatenate(ev_mul), np.concatenate(ev_w), np.concatenate(ev_sig)
+    # Merge each cell's events in application order (stable sort by cell): a zeroing
+    # event sets the cell's factor to 0 and drops the weights added before it, so
+    # the merged weight of a signal is the sum of its adds after the cell's last
+    # zeroing; signals keep the order in which they first appear on the cell, zero
+    # weights are dropped, and a cell left with none gets one (0, 0) operation.
     order = np.argsort(cell, kind="stable")
-    o_cell, o_mul, o_w, o_sig = [], [], [], []
-    k = 0
-    n = len(order)
-    while k < n:
-        c = cell[order[k]]
-        m = 1.0
-        weights: dict[int, complex] = {}
-        while k < n and cell[order[k]] == c:
-            e = order[k]
-            if ev_mul[e] == 0.0:
-                m = 0.0
-                weights = {s: 0j for s in weights}
-            else:
-                weights[ev_sig[e]] = weights.get(ev_sig[e], 0j) + ev_w[e]
-            k += 1
-        items = [(s, w) for s, w in weights.items() if w != 0] or [(0, 0j)]
-        for q, (s, w) in enumerate(items):
-            o_cell.append(c)
-            o_mul.append(m if q == 0 else 1.0)
-            o_w.append((w.real, w.imag))
-            o_sig.append(s)
+    sc, sm, sw, ss = cell[order], mul[order], wts[order], sgs[order]
+    n = len(sc)
+    start = np.r_[True, sc[1:] != sc[:-1]]
+    grp = np.cumsum(start) - 1
+    n_grp = int(grp[-1]) + 1
+    pos = np.arange(n)
+    zero = sm == 0.0
+    last_zero = np.full(n_grp, -1, dtype=np.int64)
+    np.maximum.at(last_zero, grp[zero], pos[zero])
+    has_zero = last_zero >= 0
+    adds = ~zero
+    key = grp * (int(ss.max()) + 1 if n else 1) + ss
+    ukey, first, inv = np.unique(np.where(adds, key, -1), return_index=True, return_inverse=True)
+    live = adds & (pos > last_zero[grp])
+    wsum = np.zeros(len(ukey), dtype=np.complex128)
+    np.add.at(wsum, inv[live], sw[live])
+    pair = ukey >= 0
+    p_grp, p_sig, p_first, p_w = grp[first[pair]], ss[first[pair]], first[pair], wsum[pair]
+    keep = p_w != 0
+    p_grp, p_sig, p_first, p_w = p_grp[keep], p_sig[keep], p_first[keep], p_w[keep]
+    empty_grp = np.setdiff1d(np.arange(n_grp), p_grp)
+    g_all = np.concatenate([p_grp, empty_grp])
+    f_all = np.concatenate([p_first, np.full(len(empty_grp), -1)])
+    srt = np.lexsort((f_all, g_all))
+    g_all = g_all[srt]
+    o_sig = np.concatenate([p_sig, np.zeros(len(empty_grp), dtype=np.int64)])[srt]
+    o_wc = np.concatenate([p_w, np.zeros(len(empty_grp), dtype=np.complex128)])[srt]
+    lead = np.r_[True, g_all[1:] != g_all[:-1]]
+    o_mul = np.where(lead & has_zero[g_all], 0.0, 1.0)
+    o_cell = sc[start][g_all]
+    o_w = np.stack([o_wc.real, o_wc.imag], axis=1)
     ops_cell = np.asarray(o_cell, dtype=np.int64)
     row_ptr = np.searchsorted(ops_cell // row_len, np.arange(rows + 1), side="left").astype(np.int32)
     w = np.asarray(o_w, dtype=np.float64).reshape(-1, 2)

@@ -17,6 +17,7 @@ import torch
 from .. import _native as nat
 from ..const import EPS_0, MU_0
 from .compile_ops import SourceOps, compile_monitors_2d, compile_sources
+from .graphs import capture, dft_phasors
 
 GRAPH_CHUNK = 64  # at most this many steps per captured graph
 RING_LEN = GRAPH_CHUNK  # monitor samples kept between DFT folds
@@ -80,7 +81,9 @@ class Engine2D:
         self.time_block = 1 if power else int(time_block)
         self._autotune = self._autotune and not power
         self.tb_tile = int(tb_tile)
-        self.chunk = GRAPH_CHUNK // self.time_block * self.time_block  # steps per graph
+        # steps per graph: an even number of steps keeps the copy parity, so one
+        # graph serves every chunk of a run
+        self.chunk = GRAPH_CHUNK // (2 * self.time_block) * (2 * self.time_block)
         self.n_step_launches = 0  # step-kernel launches issued (graph nodes included)
         self.n_fold_launches = 0
         g = nat.Grid2D()
@@ -169,11 +172,8 @@ class Engine2D:
         if freqs:
             self.freqs = np.concatenate(freqs)
             nf = len(self.freqs)
-            n = np.arange(self.n_steps, dtype=np.float64)
-            w = 2 * np.pi * self.freqs[None, :]
-            te, th = (n[:, None] + 1.0) * self.dt, (n[:, None] + 0.5) * self.dt
-            ph = np.stack([np.cos(w * te), -np.sin(w * te), np.cos(w * th), -np.sin(w * th)], axis=-1)
-            self.phasor = self._kept(torch.as_tensor(np.ascontiguousarray(ph)).to(self.dev))
+            self.phasor = dft_phasors(self.freqs, self.n_steps, self.dt, self.dev)
+            self.h2d_bytes += self.freqs.nbytes
             self.ring = torch.zeros((RING_LEN, self.n_designs, self.n_comp, mp.n_points, 5), dtype=self.dtype,
                                     device=self.dev)
             self.dft = torch.zeros((self.n_designs, self.n_comp, mp.n_points, nf, 5, 2), dtype=torch.float64,
@@ -266,14 +266,13 @@ class Engine2D:
         the time index comes from the device counter (d_step = first step - phase)."""
         g = self._graphs.get(phase)
         if g is None:
-            g = torch.cuda.CUDAGraph()
-            s = torch.cuda.Stream()
-            s.wait_stream(torch.cuda.current_stream())
             tb = self.time_block
-            with torch.cuda.stream(s), torch.cuda.graph(g, stream=s):
+
+            def launches():
                 for k in range(0, self.chunk, tb):
                     (self._launch_tb if tb > 1 else self._launch)(phase + k, self.d_step.data_ptr())
-            torch.cuda.current_stream().wait_stream(s)
+
+            g = capture(launches)
             self._graphs[phase] = g
         return g
 
@@ -305,7 +304,7 @@ class Engine2D:
             _TUNED[key] = min(times, key=times.get)
             self.tune_times = times
         self.time_block, self.tb_tile = _TUNED[key]
-        self.chunk = GRAPH_CHUNK // self.time_block * self.time_block
+        self.chunk = GRAPH_CHUNK // (2 * self.time_block) * (2 * self.time_block)
         self._graphs.clear()
         self._autotune = False
         return _TUNED[key]

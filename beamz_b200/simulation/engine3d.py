@@ -16,6 +16,7 @@ from .. import _native as nat
 from ..const import EPS_0, MU_0
 from ..devices.monitors import Monitor
 from .compile_ops import compile_sources
+from .graphs import capture, dft_phasors
 
 GRAPH_CHUNK = 32
 RING_LEN = GRAPH_CHUNK
@@ -155,11 +156,8 @@ class Engine3D:
         freqs = [np.asarray(m.frequencies, dtype=float) for m in self.mons if m.frequencies is not None]
         if freqs:
             self.freqs = np.concatenate(freqs)
-            n = np.arange(self.n_steps, dtype=np.float64)
-            w = 2 * np.pi * self.freqs[None, :]
-            te, th = (n[:, None] + 1.0) * self.dt, (n[:, None] + 0.5) * self.dt
-            ph = np.stack([np.cos(w * te), -np.sin(w * te), np.cos(w * th), -np.sin(w * th)], axis=-1)
-            self.phasor = self._kept(torch.as_tensor(np.ascontiguousarray(ph)).to(self.dev))
+            self.phasor = dft_phasors(self.freqs, self.n_steps, self.dt, self.dev)
+            self.h2d_bytes += self.freqs.nbytes
             self.ring = torch.zeros((RING_LEN, self.n_designs, self.n_comp, base, 6), dtype=self.dtype, device=self.dev)
             self.dft = torch.zeros((self.n_designs, self.n_comp, base, len(self.freqs), 6, 2), dtype=torch.float64,
                                    device=self.dev)
@@ -205,13 +203,11 @@ class Engine3D:
     def _graph_for(self, phase):
         g = self._graphs.get(phase)
         if g is None:
-            g = torch.cuda.CUDAGraph()
-            s = torch.cuda.Stream()
-            s.wait_stream(torch.cuda.current_stream())
-            with torch.cuda.stream(s), torch.cuda.graph(g, stream=s):
+            def launches():
                 for k in range(GRAPH_CHUNK):
                     self._launch(phase + k, self.d_step.data_ptr())
-            torch.cuda.current_stream().wait_stream(s)
+
+            g = capture(launches)
             self._graphs[phase] = g
         return g
 
