@@ -635,6 +635,7 @@ int tb_by_steps(const bz_grid2d* g, const bz_fields2d* f, const bz_source_ops* s
   switch (n_sub) {
     case 3: return tb_by_tile<T, NC, 3>(g, f, s, m, step, tile, d_step, st);
     case 7: return tb_by_tile<T, NC, 7>(g, f, s, m, step, tile, d_step, st);
+    case 9: return tb_by_tile<T, NC, 9>(g, f, s, m, step, tile, d_step, st);
     default: return tb_by_tile<T, NC, 5>(g, f, s, m, step, tile, d_step, st);
   }
 }
@@ -731,7 +732,8 @@ extern "C" int bz_step2d_multi(const bz_grid2d* g, const bz_fields2d* f, const b
                                const int64_t* d_step, void* stream) {
   const int rc = bz::check_step_args("bz_step2d_multi", g, f, s, m, step);
   if (rc != BZ_OK) return rc;
-  BZ_REQUIRE(n_sub == 1 || n_sub == 3 || n_sub == 5 || n_sub == 7, "bz_step2d_multi: n_sub must be 1, 3, 5 or 7 (got %d)",
+  BZ_REQUIRE(n_sub == 1 || n_sub == 3 || n_sub == 5 || n_sub == 7 || n_sub == 9,
+             "bz_step2d_multi: n_sub must be 1, 3, 5, 7 or 9 (got %d)",
              n_sub);
   BZ_REQUIRE(tile >= 0 && tile <= 5, "bz_step2d_multi: tile must be 0..5 (got %d)", tile);
   if (n_sub == 1) return bz_step2d(g, f, s, m, step, d_step, stream);

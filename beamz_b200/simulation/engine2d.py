@@ -22,7 +22,7 @@ from .graphs import capture, dft_phasors
 GRAPH_CHUNK = 64  # at most this many steps per captured graph
 RING_LEN = GRAPH_CHUNK  # monitor samples kept between DFT folds
 # (steps per launch, register-tile shape) tried by the autotuner
-TUNE_CANDIDATES = ((7, 0), (7, 4), (7, 5), (7, 1), (7, 3), (5, 0), (5, 4), (5, 1), (3, 1))
+TUNE_CANDIDATES = ((9, 0), (9, 5), (7, 0), (7, 4), (7, 5), (7, 1), (7, 3), (5, 0), (5, 4), (5, 1), (3, 1))
 _TUNED: dict = {}  # (device name, nx, ny, designs, components, dtype) -> (time_block, tb_tile)
 
 
@@ -75,8 +75,8 @@ class Engine2D:
         self._autotune = time_block == "auto"
         if self._autotune:
             time_block = 7
-        if int(time_block) not in (1, 3, 5, 7):
-            raise ValueError(f"time_block must be 1, 3, 5, 7 or 'auto' (got {time_block})")
+        if int(time_block) not in (1, 3, 5, 7, 9):
+            raise ValueError(f"time_block must be 1, 3, 5, 7, 9 or 'auto' (got {time_block})")
         # power accumulation runs on the single-step kernel
         self.time_block = 1 if power else int(time_block)
         self._autotune = self._autotune and not power

@@ -152,7 +152,7 @@ int bz_step2d(const bz_grid2d* g, const bz_fields2d* f, const bz_source_ops* src
  * results as n_sub bz_step2d calls from `step` (same arithmetic per cell; sources,
  * monitor records and ring samples per sub-step). Each block keeps a tile of the
  * grid in registers for all sub-steps and stores the part of it that stays exact.
- * n_sub: 1, 3, 5 or 7 (odd, so the copy read stays (step & 1) and the result lands
+ * n_sub: 1, 3, 5, 7 or 9 (odd, so the copy read stays (step & 1) and the result lands
  * in copy ((step + n_sub) & 1)); 1 is bz_step2d. tile: 0 = default (4x16), 1..5 =
  * tile shapes of 4x8, 4x16, 8x8, 5x16 and 6x12 (rows per warp x warps) for float32
  * single-component fields. Region capture (mon->region) is taken per sub-step; power

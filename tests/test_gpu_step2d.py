@@ -130,7 +130,7 @@ def _tiled_problem(bz, seed=21, n_steps=160):
     return eps, sigma, dx, dt, t, [src, g], [mv, mh], freqs
 
 
-@pytest.mark.parametrize("tb,tile", [(1, 0), (3, 1), (5, 2), (5, 3), (7, 0)])
+@pytest.mark.parametrize("tb,tile", [(1, 0), (3, 1), (5, 2), (5, 3), (7, 0), (9, 0), (9, 5)])
 @pytest.mark.parametrize("precision,tol", [("fp64", 1e-11), ("fp32", 2e-5)])
 def test_time_blocked_run_vs_oracle(bz, tb, tile, precision, tol):
     eps, sigma, dx, dt, t, srcs, mons, freqs = _tiled_problem(bz)
@@ -165,7 +165,8 @@ def test_time_blocked_batch_matches_single_steps(bz, precision):
     rng = np.random.default_rng(5)
     eps_b = np.stack([eps, eps[::-1, :], 1.0 + 11.0 * rng.random(eps.shape)])
     outs = []
-    for tb, graphs, parts in ((1, False, [150]), (5, True, [71, 64, 15]), (7, False, [150]), (3, True, [150])):
+    for tb, graphs, parts in ((1, False, [150]), (5, True, [71, 64, 15]), (7, False, [150]), (3, True, [150]),
+                              (9, True, [55, 80, 15])):
         eng = Engine2D(eps_b, sigma, dx, dx, dt, len(t), srcs, mons, precision=precision, n_comp=2, n_designs=3,
                        record=True, use_graphs=graphs, time_block=tb)
         for p in parts:
