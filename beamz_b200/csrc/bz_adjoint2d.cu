@@ -476,8 +476,8 @@ extern "C" int bz_adjoint_step2d_multi(const bz_grid2d* g, const bz_adjoint2d* s
                                        int64_t step, int32_t n_sub, int32_t phase, void* stream) {
   const int rc = bz::check_adj("bz_adjoint_step2d_multi", g, s, ops, step);
   if (rc != BZ_OK) return rc;
-  BZ_REQUIRE(n_sub == 1 || n_sub == 3 || n_sub == 5 || n_sub == 7,
-             "bz_adjoint_step2d_multi: n_sub must be 1, 3, 5 or 7 (got %d)", n_sub);
+  BZ_REQUIRE(n_sub == 1 || n_sub == 3 || n_sub == 5 || n_sub == 7 || n_sub == 9,
+             "bz_adjoint_step2d_multi: n_sub must be 1, 3, 5, 7 or 9 (got %d)", n_sub);
   BZ_REQUIRE(step + 1 >= n_sub, "bz_adjoint_step2d_multi: %d reverse steps from step %lld pass step 0", n_sub,
              (long long)step);
   if (n_sub == 1) return bz_adjoint_step2d(g, s, ops, step, phase, stream);
@@ -486,12 +486,14 @@ extern "C" int bz_adjoint_step2d_multi(const bz_grid2d* g, const bz_adjoint2d* s
     switch (n_sub) {
       case 3: return bz::launch_adj_tb<float, 3>(g, s, ops, step, phase, st);
       case 5: return bz::launch_adj_tb<float, 5>(g, s, ops, step, phase, st);
+      case 9: return bz::launch_adj_tb<float, 9>(g, s, ops, step, phase, st);
       default: return bz::launch_adj_tb<float, 7>(g, s, ops, step, phase, st);
     }
   }
   switch (n_sub) {
     case 3: return bz::launch_adj_tb<double, 3>(g, s, ops, step, phase, st);
     case 5: return bz::launch_adj_tb<double, 5>(g, s, ops, step, phase, st);
+    case 9: return bz::launch_adj_tb<double, 9>(g, s, ops, step, phase, st);
     default: return bz::launch_adj_tb<double, 7>(g, s, ops, step, phase, st);
   }
 }

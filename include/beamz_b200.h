@@ -220,7 +220,7 @@ int bz_adjoint_step2d(const bz_grid2d* g, const bz_adjoint2d* s, const bz_source
 
 /* n_sub reverse steps of bz_adjoint_step2d in one launch (step, step-1, ...,
  * step-n_sub+1; temporal blocking with the register tile of bz_step2d_multi): the same
- * gradient and operations per reverse step. n_sub: 1, 3, 5 or 7 (odd, so the copy read
+ * gradient and operations per reverse step. n_sub: 1, 3, 5, 7 or 9 (odd, so the copy read
  * is (phase & 1) and the result lands in the other copy, as n_sub single calls with
  * alternating phase leave it); step + 1 >= n_sub. */
 int bz_adjoint_step2d_multi(const bz_grid2d* g, const bz_adjoint2d* s, const bz_source_ops* ops, int64_t step,
