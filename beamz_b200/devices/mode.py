@@ -10,6 +10,8 @@ Both run once on the host when a source is created:
   run. Here the start vector is a fixed pseudo-random one and each mode is
   rotated so that its largest-magnitude entry is real and positive: the same
   modes up to a phase, reproducible across runs.
+* ``solve_modes_2d``: modes of a 2D cross-section (the optional ``cross_section``
+  solver of 3D plane sources), semi-vectorial or scalar, sparse shift-invert.
 * ``slab_mode_source``: analytic TE mode of a symmetric slab; the propagation
   constant is bracketed by a 2000-point scan of the even/odd dispersion relations
   and refined by 50 bisection steps, then the profile is normalised to unit
@@ -57,6 +59,52 @@ def solve_modes(eps, omega, dL, npml=0, m=2):
     peak = vecs[np.argmax(np.abs(vecs), axis=0), np.arange(vecs.shape[1])]
     vecs = vecs * (np.abs(peak) / np.where(peak == 0, 1.0, peak))[None, :]
     return np.sqrt(vals), vecs
+
+
+def solve_modes_2d(eps, omega, du, dv, m=1, polarization="v"):
+    """Guided modes of a 2D cross-section ``eps[nu][nv]`` (uniform steps du, dv; the
+    field is zero outside the window).
+
+    ``polarization="v"``: semi-vectorial operator for a field along v,
+    d2E/du2 + d/dv[(1/eps) d(eps E)/dv] + k0^2 eps E = beta^2 E (the eps jumps across
+    v-interfaces enter through eps at the half points, their mean); ``"scalar"``:
+    d2E/du2 + d2E/dv2 + k0^2 eps E = beta^2 E. Second-order central differences on the
+    nodes, ARPACK shift-invert around k0^2 n_max^2 with a fixed start vector. Returns
+    (neff[m], modes[m][nu][nv]) by decreasing neff, each mode of unit norm with its
+    largest entry real and positive. No counterpart in the reference, whose 3D mode
+    source multiplies two 1D slab profiles (sources.py:323-376)."""
+    eps = np.asarray(eps, dtype=float)
+    nu, nv = eps.shape
+    k0 = omega / LIGHT_SPEED
+    lap_u = sps.diags([1.0, -2.0, 1.0], [-1, 0, 1], shape=(nu, nu), format="csr", dtype=float) / du ** 2
+    A = sps.kron(lap_u, sps.identity(nv, format="csr"), format="csr")
+    if polarization == "scalar":
+        lap_v = sps.diags([1.0, -2.0, 1.0], [-1, 0, 1], shape=(nv, nv), format="csr", dtype=float) / dv ** 2
+        A = A + sps.kron(sps.identity(nu, format="csr"), lap_v, format="csr")
+    elif polarization == "v":
+        e = eps
+        e_up = np.concatenate([(e[:, 1:] + e[:, :-1]) / 2, e[:, -1:]], axis=1)  # eps at j + 1/2
+        e_dn = np.concatenate([e[:, :1], (e[:, 1:] + e[:, :-1]) / 2], axis=1)   # eps at j - 1/2
+        diag = -(e / e_up + e / e_dn) / dv ** 2
+        upper = np.zeros_like(e)
+        upper[:, :-1] = e[:, 1:] / e_up[:, :-1] / dv ** 2      # coefficient of E[j+1] in row j
+        lower = np.zeros_like(e)
+        lower[:, 1:] = e[:, :-1] / e_dn[:, 1:] / dv ** 2       # coefficient of E[j-1] in row j
+        n = nu * nv
+        A = A + sps.diags([lower.ravel()[1:], diag.ravel(), upper.ravel()[:-1]], [-1, 0, 1], shape=(n, n),
+                          format="csr")
+    else:
+        raise ValueError(f"polarization must be 'v' or 'scalar', got {polarization!r}")
+    A = A + sps.diags(k0 ** 2 * eps.ravel(), 0, format="csr")
+    v0 = np.random.default_rng(0).standard_normal(nu * nv)
+    vals, vecs = spl.eigs(A, k=m, sigma=k0 ** 2 * np.max(eps), which="LM", v0=v0)
+    order = np.argsort(-vals.real)
+    vals, vecs = vals[order], vecs[:, order]
+    vecs = vecs / np.linalg.norm(vecs, axis=0)
+    peak = vecs[np.argmax(np.abs(vecs), axis=0), np.arange(vecs.shape[1])]
+    vecs = vecs * (np.abs(peak) / np.where(peak == 0, 1.0, peak))[None, :]
+    neff = np.sqrt(np.maximum(vals.real, 0.0)) / k0  # 0 for a mode below cutoff
+    return neff, [vecs[:, i].reshape(nu, nv) for i in range(vecs.shape[1])]
 
 
 def _slab_branches(w, n_wg, n0, k0):

@@ -10,7 +10,7 @@ from __future__ import annotations
 import numpy as np
 
 from ..const import LIGHT_SPEED, µm
-from .mode import slab_mode_source, solve_modes
+from .mode import slab_mode_source, solve_modes, solve_modes_2d
 
 
 def _xyz(position):
@@ -88,7 +88,9 @@ class ModeSource:
             self.effective_indices, self.mode_vectors = solve_modes(eps_1d, self.omega, self.dL, npml=self.npml,
                                                                     m=self.num_modes)
         self.mode_profiles = []
-        if self.height and self.height > 0:
+        if self.height and self.height > 0 and mode_solver == "cross_section":
+            self.mode_profiles = self._build_3d_cross_section_profiles()
+        elif self.height and self.height > 0:
             try:
                 self.mode_profiles = self._build_3d_rect_mode_profiles() or []
             except Exception:  # noqa: BLE001 - same fallback as the reference
@@ -181,6 +183,43 @@ class ModeSource:
         plane = np.outer(np.abs(fy), np.abs(fz))
         plane /= np.max(plane) + 1e-12
         return [[[plane[iy, iz], x0, y, z] for iy, y in enumerate(ys) for iz, z in enumerate(zs)]]
+
+    def _build_3d_cross_section_profiles(self, max_points=200):
+        """Modes of the source plane's own 2D cross-section (``mode_solver="cross_section"``).
+
+        The plane (width x height, orientation yz / xz / xy) is sampled on at most
+        ``max_points`` nodes per side; ``solve_modes_2d`` finds ``num_modes`` modes, with
+        the semi-vectorial operator for a field along the height axis (z, the injected
+        Ez) for x- and y-normal planes and the scalar one for z-normal planes. Each
+        profile is scaled to peak 1 and then by (node area / dL^2), so that every grid
+        cell receives the same summed amplitude as from the reference's profiles, whose
+        points are dL apart. Sets ``effective_indices_2d``."""
+        x0, y0, z0 = self.position
+        nu = int(min(max_points, max(16, round(self.width / self.dL))))
+        nv = int(min(max_points, max(16, round(self.height / self.dL))))
+        us = np.linspace(-self.width / 2, self.width / 2, nu)
+        vs = np.linspace(-self.height / 2, self.height / 2, nv)
+        du, dv = us[1] - us[0], vs[1] - vs[0]
+        U, V = np.meshgrid(us, vs, indexing="ij")
+        orient = getattr(self, "orientation", "yz")
+        if orient == "yz":
+            X, Y, Z = np.full_like(U, x0), y0 + U, z0 + V
+        elif orient == "xz":
+            X, Y, Z = x0 + U, np.full_like(U, y0), z0 + V
+        else:
+            X, Y, Z = x0 + U, y0 + V, np.full_like(U, z0)
+        eps = np.array([[self.design.get_material_value(X[i, j], Y[i, j], Z[i, j])[0] for j in range(nv)]
+                        for i in range(nu)], dtype=float)
+        neff, modes = solve_modes_2d(eps, self.omega, du, dv, m=max(1, self.num_modes),
+                                     polarization="scalar" if orient == "xy" else "v")
+        self.effective_indices_2d = neff
+        scale = du * dv / self.dL ** 2
+        profiles = []
+        for mode in modes:
+            a = np.real(mode)
+            a = a / np.max(np.abs(a)) * scale
+            profiles.append(np.stack([a.ravel(), X.ravel(), Y.ravel(), Z.ravel()], axis=1).tolist())
+        return profiles
 
     def copy(self):
         return ModeSource(design=self.design, start=self.start, end=self.end, wavelength=self.wavelength,

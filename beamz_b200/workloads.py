@@ -90,11 +90,14 @@ def mmi_2d(nx=2000, ny=1000, dx=0.02 * µm, n_steps=20000, pml=30, mode_solver="
     return d, t, dx
 
 
-def soi_mmi_3d(nx=600, ny=300, nz=150, dx=0.02 * µm, n_steps=8000, pml=16, grid_resolution=500):
+def soi_mmi_3d(nx=600, ny=300, nz=150, dx=0.02 * µm, n_steps=8000, pml=16, grid_resolution=500,
+               mode_solver="num_eigen"):
     """600x300x150 cells at 20 nm: SiO2 box (eps 2.085) / 220 nm Si (eps 12.25) / air,
     500 nm strip into a 6 x 3 um MMI with outputs at +-0.75 um, 16-cell PML on all faces
     (the grid is built with RegularGrid3D(extrude=True)), Gaussian-pulse mode source at
-    1.55 um, DFT flux planes at 5 wavelengths on both outputs, 8000 steps."""
+    1.55 um, DFT flux planes at 5 wavelengths on both outputs, 8000 steps.
+    ``mode_solver="cross_section"`` takes the source profile from the 2D cross-section
+    eigenproblem instead of the reference's separable slab approximation."""
     W, H, Dz = (nx + 0.5) * dx, (ny + 0.5) * dx, (nz + 0.5) * dx
     d = _grade(Design(width=W, height=H, depth=Dz, material=Material(1.0), pml_size=pml * dx), pml)
     yc = H / 2
@@ -110,7 +113,8 @@ def soi_mmi_3d(nx=600, ny=300, nz=150, dx=0.02 * µm, n_steps=8000, pml=16, grid
     t = np.arange(n_steps) * courant_dt(dx, dims=3)
     sig = gaussian_pulse(t, 1.0, 30e-15, 10e-15, LIGHT_SPEED / (1.55 * µm), 0.0)
     d += ModeSource(design=d, position=(pml * dx + 0.7 * µm, yc, z_box + t_si / 2), width=1.5 * µm, height=1.0 * µm,
-                    wavelength=1.55 * µm, signal=sig, direction="+x", num_modes=1, grid_resolution=grid_resolution)
+                    wavelength=1.55 * µm, signal=sig, direction="+x", num_modes=1, grid_resolution=grid_resolution,
+                    mode_solver=mode_solver)
     x_out = W - pml * dx - 0.8 * µm
     for s, name in ((+1, "port_top"), (-1, "port_bottom")):
         d += Monitor(design=d, start=(0.0, yc + s * off - 0.6 * µm, z_box - 0.4 * µm), plane_normal="x",

@@ -181,3 +181,28 @@ def test_dft3d_flux_vs_oracle(bz):
     s = want[..., 0] * np.conj(want[..., 4]) - want[..., 1] * np.conj(want[..., 3])
     flux = 0.5 * np.real(s.reshape(len(freqs), -1).sum(axis=1)) * dx * dx
     np.testing.assert_allclose(mon.flux(), flux, rtol=1e-9)
+
+
+def test_cross_section_mode_source_run_vs_oracle(bz):
+    """A 3D run driven by a ModeSource with mode_solver="cross_section" (its profile from
+    the 2D cross-section eigenproblem) against the oracle's run of the same source."""
+    d = bz.Design(width=3e-6, height=2e-6, depth=1.2e-6, material=bz.Material(permittivity=2.085), auto_pml=False)
+    d.add(bz.Rectangle(position=(0, 0.75e-6, 0.5e-6), width=3e-6, height=0.5e-6, depth=0.22e-6,
+                       material=bz.Material(permittivity=12.25)))
+    dx = 50e-9
+    dt = 0.99 * dx / (bz.LIGHT_SPEED * np.sqrt(3))
+    t = np.arange(60) * dt
+    sig = bz.ramped_cosine(t, amplitude=1.0, frequency=bz.LIGHT_SPEED / 1.55e-6, phase=0, ramp_duration=10 * dt,
+                           t_max=t[-1])
+    src = bz.ModeSource(design=d, position=(0.6e-6, 1.0e-6, 0.61e-6), width=1.2e-6, height=0.8e-6,
+                        wavelength=1.55e-6, signal=sig, direction="+x", num_modes=1, mode_solver="cross_section")
+    grid = bz.RegularGrid3D(d, dx, extrude=True)
+    eps, sig_grid = grid.permittivity.copy(), grid.conductivity.copy()
+    sim = bz.FDTD(design=grid, time=t, backend_options={"precision": "fp64", "n_comp": 1})
+    sim.sources = [src]
+    sim.run(live=False, save=False, save_memory_mode=True)
+    ref = fdtd3d.run(eps, sig_grid, dx, dx, dx, dt, len(t), [src], [])
+    for k in KEYS:
+        got = sim.engine.field(k).cpu().numpy()
+        assert np.abs(got).max() > 0, k
+        assert rel_l2(got, np.real(ref["fields"][k])) <= 1e-11, k
