@@ -4,8 +4,8 @@ A Design holds, in painter's order, a background rectangle followed by the
 structures, sources and monitors added to it, plus the absorbing boundaries.
 With ``auto_pml`` it adds four edge strips and four corner regions of
 thickness ``pml_size`` and four display-only rectangles flagged ``is_pml``.
-GDS import/export and polygon union (core.py:159-553) need gdspy/shapely and are
-not provided.
+GDS import/export (core.py:445-553) reads and writes the GDSII stream itself
+(``design/gds.py``); polygon union (core.py:159-440) needs shapely and is not provided.
 """
 from __future__ import annotations
 
@@ -149,11 +149,54 @@ class Design:
     def unify_polygons(self):
         raise NotImplementedError("polygon union needs shapely, which beamz_b200 does not use")
 
-    def import_gds(self, *args, **kwargs):
-        raise NotImplementedError("GDS I/O needs gdspy, which beamz_b200 does not use")
+    @staticmethod
+    def import_gds(gds_file: str, default_depth=1e-6):
+        """New Design holding every polygon of the file's flattened top cells
+        (core.py:445-478): ``layers[layer]`` lists the polygons of each GDS layer, all
+        with ``default_depth`` (a positive depth makes the design 3D). The polygons carry
+        no material, as in the reference. Read by ``design/gds.py``."""
+        from .gds import read_gds
 
-    def export_gds(self, *args, **kwargs):
-        raise NotImplementedError("GDS I/O needs gdspy, which beamz_b200 does not use")
+        design = Design()
+        n = 0
+        for (layer, _datatype), polys in read_gds(gds_file).items():
+            design.layers.setdefault(layer, [])
+            for pts in polys:
+                poly = Polygon(vertices=[(float(x), float(y)) for x, y in pts], depth=default_depth)
+                design.layers[layer].append(poly)
+                design.structures.append(poly)
+                n += 1
+        if default_depth > 0:
+            design.is_3d = True
+            design.depth = default_depth
+        display_status(f"Imported {n} polygons from '{gds_file}' into Design object.")
+        return design
+
+    def export_gds(self, output_file):
+        """Writes the structures (not sources, monitors or PML strips) as GDS polygons,
+        one layer per distinct (permittivity, permeability, conductivity) in order of
+        first appearance, as core.py:480-553 does; user unit 1 um, database unit 1 nm,
+        cell "main". Unlike the reference, touching polygons of one material are not
+        merged first (that union needs shapely); each structure is its own boundary,
+        holes written as keyholes."""
+        from .gds import write_gds
+
+        groups: dict = {}
+        for st in self.structures:
+            if getattr(st, "is_pml", False) or not isinstance(st, Polygon):
+                continue
+            mat = getattr(st, "material", None)
+            if mat is None or not st.vertices:
+                continue
+            key = (getattr(mat, "permittivity", 1.0), getattr(mat, "permeability", 1.0),
+                   getattr(mat, "conductivity", 0.0))
+            outline = np.asarray([(v[0], v[1]) for v in st.vertices], dtype=float)
+            holes = [np.asarray([(v[0], v[1]) for v in h], dtype=float) for h in getattr(st, "interiors", []) if h]
+            groups.setdefault(key, []).append((outline, holes))
+        write_gds(output_file, {layer: polys for layer, polys in enumerate(groups.values())})
+        display_status(f"GDS file saved as '{output_file}' with {len(groups)} material-based layers")
+        for layer, key in enumerate(groups):
+            display_status(f"Layer {layer}: eps_r={key[0]:.1f}, mu_r={key[1]:.1f}, sigma={key[2]:.2e} S/m")
 
 
 # Circle, Ring and CircularBend are Polygon subclasses, so get_material_value's
