@@ -9,8 +9,6 @@ chunks when no host work is due between steps.
 """
 from __future__ import annotations
 
-import ctypes as C
-
 import numpy as np
 import torch
 

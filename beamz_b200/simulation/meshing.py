@@ -13,7 +13,6 @@ slice semantics) and tabulates the position-only part of each PML region
 from __future__ import annotations
 
 import ctypes as C
-import math
 from typing import Any
 
 import numpy as np
