@@ -289,6 +289,22 @@ __global__ void __launch_bounds__(32 * NW) step2d_tb_kernel(
   __shared__ T s_bot[NW][NC][TW];  // last row's new Hy of each warp
   __shared__ int s_src[TH][2], s_mon[TH][2];  // op ranges of each tile row
 
+  // row pointers of the op lists first, so their latency overlaps the tile loads
+  int rs_lo = 0, rs_hi = 0, rm_lo = 0, rm_hi = 0;
+  if (lane < R) {
+    const int y = yb + lane;
+    if (y >= 0 && y < ny) {
+      if (o.n_src > 0) {
+        rs_lo = __ldg(o.src_row + y);
+        rs_hi = __ldg(o.src_row + y + 1);
+      }
+      if (o.n_mon > 0) {
+        rm_lo = __ldg(o.mon_row + y);
+        rm_hi = __ldg(o.mon_row + y + 1);
+      }
+    }
+  }
+
   int xs[2];
   xs[0] = X0 + lane;
   xs[1] = X0 + 32 + lane;
@@ -329,14 +345,14 @@ __global__ void __launch_bounds__(32 * NW) step2d_tb_kernel(
     int s0 = 0, s1 = 0, m0 = 0, m1 = 0;
     if (y >= 0 && y < ny) {
       if (o.n_src > 0) {
-        const int lo = __ldg(o.src_row + y), hi = __ldg(o.src_row + y + 1);
+        const int lo = rs_lo, hi = rs_hi;
         if (lo < hi) {
           s0 = lower_bound_i(o.src_cell, lo, hi, y * nx + max(X0, 0));
           s1 = lower_bound_i(o.src_cell, s0, hi, y * nx + min(X0 + TW, nx));
         }
       }
       if (o.n_mon > 0 && tr >= TS && tr < TH - TS) {
-        const int lo = __ldg(o.mon_row + y), hi = __ldg(o.mon_row + y + 1);
+        const int lo = rm_lo, hi = rm_hi;
         if (lo < hi) {
           m0 = lower_bound_i(o.mon_cell, lo, hi, y * nx + X0 + TS);
           m1 = lower_bound_i(o.mon_cell, m0, hi, y * nx + min(X0 + TW - TS, nx));
