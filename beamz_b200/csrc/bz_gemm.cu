@@ -473,7 +473,7 @@ int launch_gemm_tc(const GemmP& p, cudaStream_t st) {
 }
 
 
-// ---- tcgen05 + TMA path (batch 1): one control thread, two-stage pipeline ---------
+// ---- tcgen05 + TMA path (batch 1): one control thread, four-stage pipeline --------
 // Operand stages are filled by TMA tiled copies with 128-byte swizzling (2D tensor
 // maps over the row-major K-contiguous A and B, box 64 elements x 128 or 256 rows: one
 // copy per operand per stage), which is the K-major SWIZZLE_128B layout of the MMA
@@ -481,10 +481,12 @@ int launch_gemm_tc(const GemmP& p, cudaStream_t st) {
 // elements advances the start address by 32 bytes inside the atom). Thread 0 waits for
 // a stage's copies (mbarrier complete_tx), issues its four MMAs, commits them to the
 // stage's "empty" barrier, and refills the previous stage once its MMAs are done, so
-// the tensor pipe always has queued work. 96 KB of stages: two CTAs per SM, one's
-// epilogue overlapping the other's main loop. Bounded waits as above.
+// the tensor pipe always has queued work. Four 48 KB stages (192 KB, one CTA per SM)
+// keep three tiles of loads in flight behind the MMAs: with two, the next tile's load
+// latency (about a microsecond) outlasted a tile's MMAs and the tensor pipe idled.
+// Bounded waits as above.
 namespace tma {
-constexpr int S = 2, BK = 64;
+constexpr int S = 4, BK = 64;
 constexpr int A_ST = tc::BM * BK * 2, B_ST = tc::BN * BK * 2, STAGE = A_ST + B_ST;
 constexpr int SMEM = S * STAGE + 1024 + 128;  // + alignment slack + barriers
 }  // namespace tma
