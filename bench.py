@@ -52,22 +52,27 @@ def parse():
     p.add_argument("--iterations", type=int, default=15, help="surrogate_2d: plain-adjoint ascent iterations")
     p.add_argument("--designs", type=int, default=64, help="topo_2d: designs per batch")
     p.add_argument("--time-steps", type=int, default=None, help="override the workload's step count")
+    p.add_argument("--nz", type=int, default=None, help="soi_mmi_3d: z planes (default 150; smaller for profiling)")
     p.add_argument("--cpu-steps", type=int, default=60, help="time steps of the CPU baseline sample")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--n-comp", type=int, default=1, help="field components: 1 = real (physical) field, 2 = Re+Im")
     return p.parse_args()
 
 
-def workload(name, n_steps=None):
+def workload(name, n_steps=None, nz=None):
     from beamz_b200 import workloads as W
 
     kw = {} if n_steps is None else {"n_steps": n_steps}
+    if nz is not None and name == "soi_mmi_3d":
+        kw["nz"] = nz  # thinner 3D grid (profiling cases)
     d, t, dx = getattr(W, name)(**kw)
     desc = {"mmi_2d": "2D TE 1x2 MMI splitter, 2000x1000 cells at 20 nm, 30-cell PML, CW mode source, "
                       "5-wavelength DFT flux monitors",
             "dipole_2d": "2D point dipole in vacuum, 400x400 cells at 20 nm, 20-cell PML, 4 edge monitors",
             "soi_mmi_3d": "3D SOI strip into a 6x3 um MMI, 600x300x150 cells at 20 nm, 16-cell PML on all faces, "
                           "Gaussian-pulse mode source, 5-wavelength DFT flux planes on both outputs"}[name]
+    if nz is not None and name == "soi_mmi_3d":
+        desc += f" (here {nz} z planes)"
     return d, t, dx, desc
 
 
@@ -184,7 +189,7 @@ def run_b200(args):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     from beamz_b200 import FDTD, RegularGrid, RegularGrid3D
 
-    d, t, dx, desc = workload(args.workload, args.time_steps)
+    d, t, dx, desc = workload(args.workload, args.time_steps, args.nz)
     is3d = bool(d.is_3d and d.depth)
     grid = RegularGrid3D(d, dx, extrude=True) if is3d else RegularGrid(d, dx)
     shape = grid.permittivity.shape
