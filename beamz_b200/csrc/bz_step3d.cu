@@ -13,7 +13,9 @@
 //      H(k-1) is carried in registers from the previous plane;
 //   4. owned threads compute E(k) and write H(k), E(k).
 // The first plane's H(k-1) is recomputed from global memory. Ping-pong copies
-// keep every launch reading only the previous step's values.
+// keep every launch reading only the previous step's values. Float32 fields with
+// one component (real fields) take step3d_pair_kernel, the same schedule with two
+// x cells per thread.
 #include "bz_internal.cuh"
 
 namespace bz {
@@ -252,6 +254,208 @@ int launch3d(const bz_grid3d* gd, const bz_fields3d* f, int64_t step, cudaStream
   return check_launch("bz_step3d");
 }
 
+// ---------------------------------------------------------------------------- paired columns (float32, one component)
+// The same step with two adjacent x cells per thread, moved as float2: a warp spans 64
+// columns whose first two (one pair, to keep 8-byte alignment) are the halo shared
+// with the neighbouring tile, so a block owns 62 x (TY-1) columns. Loads, stores,
+// shared-memory traffic, shuffles, barriers and index arithmetic are issued once per
+// pair. The pair (x, x+1) starts at an even x; when nx is odd the last pair's second
+// cell is row padding (pitch > nx), read but never stored, and no stored value
+// depends on it.
+__device__ __forceinline__ float2 ld2(const float* p, long long i, bool ok) {
+  return ok ? __ldg(reinterpret_cast<const float2*>(p + i)) : make_float2(0.f, 0.f);
+}
+
+// Stores both cells when the second exists (then so does the first), else the first alone.
+__device__ __forceinline__ void st2(float* p, long long i, float2 v, bool s0, bool s1) {
+  if (s1)
+    *reinterpret_cast<float2*>(p + i) = v;
+  else if (s0)
+    p[i] = v.x;
+}
+
+struct PairIn {
+  float2 hx, hy, hz, a, ce, ez_y, ex_y;
+  float ez_x, ey_x;  // E at x+2 (the warp's last lane)
+};
+
+template <int ZB, int TY>
+__global__ void __launch_bounds__(TX * TY) step3d_pair_kernel(Ptr3<float> in, Out3<float> out,
+                                                               const float* __restrict__ ce,
+                                                               const float* __restrict__ loss, Geo3D<float> g) {
+  __shared__ float2 s_ez[TY][TX], s_ex[TY][TX], s_hz[TY][TX], s_hx[TY][TX];
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  const int nx = g.nx, ny = g.ny, nz = g.nz;
+  const int x = blockIdx.x * (2 * TX - 2) - 2 + 2 * tx;  // first cell of the pair
+  const int y = blockIdx.y * (TY - 1) - 1 + ty;
+  const int d = blockIdx.z / g.nzb;
+  const int z0 = (blockIdx.z - d * g.nzb) * ZB;
+  const int z1 = min(z0 + ZB, nz);
+  const bool xin = x >= 0 && x < nx, yin = y >= 0 && y < ny, inb = xin && yin;
+  const bool owned = inb && tx >= 1 && ty >= 1;
+  const bool xe = tx == TX - 1, ye = ty == TY - 1;
+  const bool xnb = yin && x + 2 < nx, ynb = xin && y + 1 < ny;
+  // which cells of the pair exist in each component's extent, and which are updated
+  const bool x0m = x <= nx - 2, x1m = x + 1 <= nx - 2, x1in = x + 1 <= nx - 1, x0p = x >= 1;
+  const bool yint = y >= 1 && y <= ny - 2, ym = y <= ny - 2;
+  const long long P = g.plane;
+  const long long mb = (g.n_mat > 1 ? (long long)d : 0LL) * g.vol;
+  const long long col = (long long)y * g.pitch + x;
+  const long long fb = (long long)d * g.vol;
+
+  auto load_plane = [&](int k, PairIn& q) {
+    const long long po = (long long)k * P + col;
+    q.a = ld2(loss + mb, po, inb);
+    q.ce = ld2(ce + mb, po, inb);
+    const long long o = fb + po;
+    q.hx = ld2(in.h[0], o, inb);
+    q.hy = ld2(in.h[1], o, inb);
+    q.hz = ld2(in.h[2], o, inb);
+    q.ez_x = ld(in.e[2], o + 2, xe && xnb);
+    q.ey_x = ld(in.e[1], o + 2, xe && xnb);
+    q.ez_y = ld2(in.e[2], o + g.pitch, ye && ynb);
+    q.ex_y = ld2(in.e[0], o + g.pitch, ye && ynb);
+  };
+
+  float2 exk, eyk, ezk, exn, eyn, ezn, hxm = make_float2(0.f, 0.f), hym = make_float2(0.f, 0.f);
+  PairIn cur, nxt;
+  load_plane(z0, cur);
+  {
+    const long long o = fb + (long long)z0 * P + col;
+    exk = ld2(in.e[0], o, inb);
+    eyk = ld2(in.e[1], o, inb);
+    ezk = ld2(in.e[2], o, inb);
+    exn = ld2(in.e[0], o + P, inb && z0 + 1 < nz);
+    eyn = ld2(in.e[1], o + P, inb && z0 + 1 < nz);
+    ezn = ld2(in.e[2], o + P, inb && z0 + 1 < nz);
+  }
+  if (z0 >= 1 && inb) {  // H(z0-1) of the pair, recomputed from global memory
+    const long long po = (long long)(z0 - 1) * P + col, o = fb + po;
+    const float2 a = __ldg(reinterpret_cast<const float2*>(loss + mb + po));
+    const float2 ez = ld2(in.e[2], o, true), ex = ld2(in.e[0], o, true), ey = ld2(in.e[1], o, true);
+    const float2 ez_yp = ld2(in.e[2], o + g.pitch, y + 1 < ny);
+    const float ez_x2 = ld(in.e[2], o + 2, x + 2 < nx);
+    const float2 hx = ld2(in.h[0], o, true), hy = ld2(in.h[1], o, true);
+    float fh, cx, cy, cz;
+    hfac(a.x, g, fh, cx, cy, cz);
+    hxm.x = fh * hx.x - (cy * (ez_yp.x - ez.x) - cz * (eyk.x - ey.x));
+    hym.x = fh * hy.x - (cz * (exk.x - ex.x) - cx * (ez.y - ez.x));
+    hfac(a.y, g, fh, cx, cy, cz);
+    hxm.y = fh * hx.y - (cy * (ez_yp.y - ez.y) - cz * (eyk.y - ey.y));
+    hym.y = fh * hy.y - (cz * (exk.y - ex.y) - cx * (ez_x2 - ez.y));
+  }
+
+  for (int k = z0; k < z1; ++k) {
+    const long long po = (long long)k * P + col;
+    float2 ex2, ey2, ez2;  // prefetch: inputs of plane k+1 and E(k+2)
+    if (k + 1 < z1) {
+      load_plane(k + 1, nxt);
+      const long long o = fb + po + 2 * P;
+      ex2 = ld2(in.e[0], o, inb && k + 2 < nz);
+      ey2 = ld2(in.e[1], o, inb && k + 2 < nz);
+      ez2 = ld2(in.e[2], o, inb && k + 2 < nz);
+    }
+    float fh0, cx0, cy0, cz0, fh1, cx1, cy1, cz1;
+    hfac(cur.a.x, g, fh0, cx0, cy0, cz0);
+    hfac(cur.a.y, g, fh1, cx1, cy1, cz1);
+    s_ez[ty][tx] = ezk;
+    s_ex[ty][tx] = exk;
+    __syncthreads();
+    const float2 ez_yp = ye ? cur.ez_y : s_ez[ty + (ye ? 0 : 1)][tx];
+    const float2 ex_yp = ye ? cur.ex_y : s_ex[ty + (ye ? 0 : 1)][tx];
+    float ez_x2 = __shfl_down_sync(FULL, ezk.x, 1);
+    float ey_x2 = __shfl_down_sync(FULL, eyk.x, 1);
+    if (xe) {
+      ez_x2 = cur.ez_x;
+      ey_x2 = cur.ey_x;
+    }
+    float2 hxn, hyn, hzn;
+    hxn.x = fh0 * cur.hx.x - (cy0 * (ez_yp.x - ezk.x) - cz0 * (eyn.x - eyk.x));
+    hyn.x = fh0 * cur.hy.x - (cz0 * (exn.x - exk.x) - cx0 * (ezk.y - ezk.x));
+    hzn.x = fh0 * cur.hz.x - (cx0 * (eyk.y - eyk.x) - cy0 * (ex_yp.x - exk.x));
+    hxn.y = fh1 * cur.hx.y - (cy1 * (ez_yp.y - ezk.y) - cz1 * (eyn.y - eyk.y));
+    hyn.y = fh1 * cur.hy.y - (cz1 * (exn.y - exk.y) - cx1 * (ez_x2 - ezk.y));
+    hzn.y = fh1 * cur.hz.y - (cx1 * (ey_x2 - eyk.y) - cy1 * (ex_yp.y - exk.y));
+    s_hz[ty][tx] = hzn;
+    s_hx[ty][tx] = hxn;
+    __syncthreads();
+    const float hy_xm = __shfl_up_sync(FULL, hyn.y, 1);
+    const float hz_xm = __shfl_up_sync(FULL, hzn.y, 1);
+    if (owned) {
+      const long long o = fb + po;
+      const float2 hz_ym = s_hz[ty - 1][tx];
+      const float2 hx_ym = s_hx[ty - 1][tx];
+      const bool kin = k >= 1 && k <= nz - 2, kz = k <= nz - 2;
+      const float cv0 = cur.ce.x, cv1 = cur.ce.y;
+      const float fe0 = 1.f - cur.a.x * cv0 * g.inv_kd2, fe1 = 1.f - cur.a.y * cv1 * g.inv_kd2;
+      float2 ex = exk, ey = eyk, ez = ezk;
+      if (kin && yint && x0m) ex.x = fe0 * exk.x + cv0 * ((hzn.x - hz_ym.x) - g.qz * (hyn.x - hym.x));
+      if (kin && yint && x1m) ex.y = fe1 * exk.y + cv1 * ((hzn.y - hz_ym.y) - g.qz * (hyn.y - hym.y));
+      if (kin && ym && x0p && x0m) ey.x = fe0 * eyk.x + cv0 * (g.qz * (hxn.x - hxm.x) - g.qx * (hzn.x - hz_xm));
+      if (kin && ym && x1m) ey.y = fe1 * eyk.y + cv1 * (g.qz * (hxn.y - hxm.y) - g.qx * (hzn.y - hzn.x));
+      if (kz && yint && x0p && x0m) ez.x = fe0 * ezk.x + cv0 * (g.qx * (hyn.x - hy_xm) - (hxn.x - hx_ym.x));
+      if (kz && yint && x1m) ez.y = fe1 * ezk.y + cv1 * (g.qx * (hyn.y - hyn.x) - (hxn.y - hx_ym.y));
+      st2(out.e[0], o, ex, x0m, x1m);
+      st2(out.e[1], o, ey, ym, ym && x1in);
+      st2(out.e[2], o, ez, kz, kz && x1in);
+      st2(out.h[0], o, hxn, kz && ym, kz && ym && x1in);
+      st2(out.h[1], o, hyn, kz && x0m, kz && x1m);
+      st2(out.h[2], o, hzn, ym && x0m, ym && x1m);
+    }
+    exk = exn;
+    eyk = eyn;
+    ezk = ezn;
+    exn = ex2;
+    eyn = ey2;
+    ezn = ez2;
+    hxm = hxn;
+    hym = hyn;
+    cur = nxt;
+  }
+}
+
+template <int ZB, int TY>
+int launch3d_pair(const bz_grid3d* gd, const bz_fields3d* f, int64_t step, cudaStream_t st) {
+  Geo3D<float> g;
+  g.nx = gd->nx;
+  g.ny = gd->ny;
+  g.nz = gd->nz;
+  g.pitch = gd->pitch;
+  g.n_designs = gd->n_designs;
+  g.n_mat = gd->n_mat;
+  g.nzb = (int)ceil_div(gd->nz, ZB);
+  g.plane = (long long)gd->ny * gd->pitch;
+  g.vol = g.plane * gd->nz;
+  g.chx = (float)gd->chx;
+  g.chy = (float)gd->chy;
+  g.chz = (float)gd->chz;
+  g.qx = (float)gd->qx;
+  g.qz = (float)gd->qz;
+  g.inv_kd2 = (float)gd->inv_kd2;
+  const int src = (int)(step & 1);
+  Ptr3<float> in;
+  Out3<float> out;
+  for (int i = 0; i < 3; ++i) {
+    in.e[i] = (const float*)f->e[src][i];
+    in.h[i] = (const float*)f->h[src][i];
+    out.e[i] = (float*)f->e[src ^ 1][i];
+    out.h[i] = (float*)f->h[src ^ 1][i];
+  }
+  dim3 block(TX, TY);
+  dim3 grid((unsigned)ceil_div(gd->nx, 2 * TX - 2), (unsigned)ceil_div(gd->ny, TY - 1),
+            (unsigned)(g.nzb * gd->n_designs));
+  step3d_pair_kernel<ZB, TY><<<grid, block, 0, st>>>(in, out, (const float*)f->ce, (const float*)f->loss, g);
+  return check_launch("bz_step3d");
+}
+
+// float2 accesses need every array 8-byte aligned (offsets are even: pitch % 32 == 0).
+inline bool pair_aligned(const bz_fields3d* f) {
+  bool ok = ((uintptr_t)f->ce | (uintptr_t)f->loss) % 8 == 0;
+  for (int c = 0; c < 2; ++c)
+    for (int i = 0; i < 3; ++i) ok = ok && ((uintptr_t)f->e[c][i] | (uintptr_t)f->h[c][i]) % 8 == 0;
+  return ok;
+}
+
 template <typename T, int TY>
 int dispatch3d_ty(const bz_grid3d* g, const bz_fields3d* f, int64_t step, cudaStream_t st) {
   const bool z8 = g->tile_z == 8;
@@ -261,6 +465,11 @@ int dispatch3d_ty(const bz_grid3d* g, const bz_fields3d* f, int64_t step, cudaSt
 
 template <typename T>
 int dispatch3d(const bz_grid3d* g, const bz_fields3d* f, int64_t step, cudaStream_t st) {
+  if (sizeof(T) == 4 && g->n_comp == 1 && pair_aligned(f)) {
+    const bool z8 = g->tile_z == 8;
+    if (g->tile_y == 16) return z8 ? launch3d_pair<8, 16>(g, f, step, st) : launch3d_pair<16, 16>(g, f, step, st);
+    return z8 ? launch3d_pair<8, 8>(g, f, step, st) : launch3d_pair<16, 8>(g, f, step, st);
+  }
   return g->tile_y == 16 ? dispatch3d_ty<T, 16>(g, f, step, st) : dispatch3d_ty<T, 8>(g, f, step, st);
 }
 

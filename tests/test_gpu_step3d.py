@@ -79,9 +79,9 @@ def test_step3d_matches_reference_run(bz, golden, precision, tol):
         assert np.abs(np.real(np.asarray(m.power_history)) - want_p).max() <= 10 * tol * np.abs(want_p).max()
 
 
-def _odd_problem(bz, n_steps=50, seed=4):
+def _odd_problem(bz, n_steps=50, seed=4, shape=(9, 11, 13)):
     rng = np.random.default_rng(seed)
-    nz, ny, nx = 9, 11, 13
+    nz, ny, nx = shape
     dx = 30e-9
     eps = 1.0 + 9.0 * rng.random((nz, ny, nx))
     sig = np.zeros((nz, ny, nx))
@@ -103,11 +103,13 @@ def _odd_problem(bz, n_steps=50, seed=4):
     return d, grid, eps, sig, dx, dt, t, src, sgn
 
 
-@pytest.mark.parametrize("precision,tol", [("fp64", 1e-11), ("fp32", 2e-5)])
-def test_step3d_odd_grid_complex_vs_oracle(bz, precision, tol):
+@pytest.mark.parametrize("precision,tol,tile_y", [("fp64", 1e-11, 8), ("fp32", 2e-5, 8), ("fp64", 1e-11, 16),
+                                                   ("fp32", 2e-5, 16)])
+def test_step3d_odd_grid_complex_vs_oracle(bz, precision, tol, tile_y):
+    """Two-component (complex) fields; fp64 with 16-row tiles needs 64 KB of shared memory."""
     d, grid, eps, sig, dx, dt, t, src, _ = _odd_problem(bz)
     mon = bz.Monitor(design=d, start=(1 * dx, 1 * dx, 4 * dx), end=(11 * dx, 9 * dx, 4 * dx))
-    sim = bz.FDTD(design=grid, time=t, devices=[mon], backend_options={"precision": precision})
+    sim = bz.FDTD(design=grid, time=t, devices=[mon], backend_options={"precision": precision, "tile_y": tile_y})
     sim.sources = [src]
     sim.run(live=False, save=False, save_memory_mode=True, accumulate_power=True)
     ref = fdtd3d.run(eps, sig, dx, dx, dx, dt, len(t), [src], [mon], accumulate_power=True)
@@ -119,6 +121,25 @@ def test_step3d_odd_grid_complex_vs_oracle(bz, precision, tol):
     got = np.array(mon.fields["Ez"])
     want = ref["records"][0]["fields"]["Ez"]
     assert np.abs(got - want).max() <= tol * np.abs(want).max()
+
+
+@pytest.mark.parametrize("shape", [(9, 11, 13), (12, 17, 131), (10, 9, 128)])
+@pytest.mark.parametrize("tile_z,tile_y", [(16, 8), (8, 8), (16, 16), (8, 16)])
+def test_step3d_real_fp32_vs_oracle(bz, shape, tile_z, tile_y):
+    """Real float32 fields (stepped two x cells per thread): odd nx (the last pair ends in
+    row padding), several x tiles (62 owned columns each), several z blocks."""
+    d, grid, eps, sig, dx, dt, t, _, sgn = _odd_problem(bz, shape=shape)
+    nz, ny, nx = shape
+    g = bz.GaussianSource(position=((nx - 3) * dx, 5 * dx, 4 * dx), width=dx / 10, signal=sgn)
+    g2 = bz.GaussianSource(position=(2 * dx, (ny - 3) * dx, (nz - 4) * dx), width=dx / 10, signal=sgn)
+    sim = bz.FDTD(design=grid, time=t, backend_options={"precision": "fp32", "tile_z": tile_z, "tile_y": tile_y})
+    sim.sources = [g, g2]
+    sim.run(live=False, save=False, save_memory_mode=True)
+    assert sim.engine.n_comp == 1
+    ref = fdtd3d.run(eps, sig, dx, dx, dx, dt, len(t), [g, g2], [])
+    for k in KEYS:
+        got = sim.engine.field(k).cpu().numpy()
+        assert rel_l2(got, ref["fields"][k]) <= 2e-5, (k, rel_l2(got, ref["fields"][k]))
 
 
 def test_step3d_graph_equals_direct(bz):
@@ -157,12 +178,13 @@ def test_step3d_tile_heights_agree(bz):
     d, grid, eps, sig, dx, dt, t, src, sgn = _odd_problem(bz, n_steps=60)
     g = bz.GaussianSource(position=(6 * dx, 5 * dx, 4 * dx), width=dx / 10, signal=sgn)
     outs = []
-    for tz in (16, 8):
-        sim = bz.FDTD(design=grid, time=t, backend_options={"tile_z": tz})
+    for tz, ty in ((16, 8), (8, 8), (16, 16), (8, 16)):
+        sim = bz.FDTD(design=grid, time=t, backend_options={"tile_z": tz, "tile_y": ty})
         sim.sources = [g]
         sim.run(live=False, save=False, save_memory_mode=True)
         outs.append(sim.engine.field("Ey").cpu().numpy())
-    assert rel_l2(outs[1], outs[0]) <= 1e-6
+    for o in outs[1:]:
+        assert rel_l2(o, outs[0]) <= 1e-6
 
 
 def test_dft3d_flux_vs_oracle(bz):
