@@ -211,17 +211,29 @@ class FDTD:
         self.current_step += 1
         return True
 
+    def _next_save(self, step: int) -> int:
+        """First step >= ``step`` for which _save_due holds (num_steps if none does)."""
+        n = self.num_steps
+        full = self._save_results and not self.save_memory_mode
+        cache = bool(self._save_results and self._cache_fields)
+        if step >= n or not (full or cache):
+            return n
+        nxt = n - 1  # the last step is always saved
+        for on, f in ((full, self._effective_save_freq), (cache, self._cache_frequency)):
+            if on:
+                f = max(1, int(f))
+                nxt = min(nxt, -(-step // f) * f)
+        return nxt
+
     def _run_until_end(self):
         """Steps to the end, in graph chunks between the steps that need host copies."""
         while self.current_step < self.num_steps:
-            nxt = self.current_step
-            while nxt < self.num_steps and not self._save_due(nxt):
-                nxt += 1
-            n_free = nxt - self.current_step
+            n_free = self._next_save(self.current_step) - self.current_step
             if n_free > 0:
                 self.engine.run_steps(n_free)
-                for _ in range(n_free):
-                    self.t += self.dt
+                # t advances by repeated addition, as one step at a time would
+                # (accumulate adds in order, so the rounding is the same)
+                self.t = float(np.add.accumulate(np.r_[self.t, np.full(n_free, self.dt)])[-1])
                 self.current_step += n_free
             if self.current_step < self.num_steps:
                 self.step()

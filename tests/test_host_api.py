@@ -155,3 +155,29 @@ def test_masked_blur_and_adam():
     np.testing.assert_allclose(u, [-0.1, 0.1], rtol=1e-6)
     with pytest.raises(ValueError):
         Optimizer(method="sgd")
+
+
+@pytest.mark.parametrize("save,memory,cache,decimate,n", [(False, True, [], 1, 20000), (True, False, [], 1, 20000),
+                                                          (True, True, ["Ez"], 1, 5000), (True, False, [], 3, 997),
+                                                          (True, False, ["Hx"], 2, 123), (True, True, [], 1, 50)])
+def test_next_save_step_matches_per_step_scan(bz, save, memory, cache, decimate, n):
+    """FDTD._next_save gives the step a scan with _save_due stops at, from every start."""
+    sim = bz.FDTD.__new__(bz.FDTD)
+    freq = (max(10, n // 100) if save else 1) * decimate
+    sim.__dict__.update(num_steps=n, _save_results=save, save_memory_mode=memory, _cache_fields=list(cache),
+                        _effective_save_freq=freq, _cache_frequency=1 if cache else freq)
+    starts = range(n + 1) if n <= 1000 else list(range(0, 400)) + list(range(n - 400, n + 1))
+    for s in starts:
+        want = s
+        while want < n and not sim._save_due(want):
+            want += 1
+        assert sim._next_save(s) == want, s
+
+
+def test_time_accumulation_matches_repeated_addition():
+    dt = 2.3456789e-17
+    t_loop = 1.0e-15
+    for _ in range(20000):
+        t_loop += dt
+    t_acc = float(np.add.accumulate(np.r_[1.0e-15, np.full(20000, dt)])[-1])
+    assert t_acc == t_loop
