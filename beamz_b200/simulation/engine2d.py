@@ -9,6 +9,8 @@ chunks when no host work is due between steps.
 """
 from __future__ import annotations
 
+import warnings
+
 import numpy as np
 import torch
 
@@ -103,7 +105,10 @@ class Engine2D:
         eps_r = np.ascontiguousarray(np.broadcast_to(np.asarray(eps_r, dtype=np.float64), shape))
         sigma = np.ascontiguousarray(np.broadcast_to(np.asarray(sigma, dtype=np.float64), shape))
         self.h2d_bytes += eps_r.nbytes + sigma.nbytes
-        self.set_material_tensors(torch.as_tensor(eps_r).to(self.dev), torch.as_tensor(sigma).to(self.dev))
+        with warnings.catch_warnings():  # a read-only broadcast view is only read by the copy
+            warnings.filterwarnings("ignore", message="The given NumPy array is not writable")
+            te, ts = torch.as_tensor(eps_r).to(self.dev), torch.as_tensor(sigma).to(self.dev)
+        self.set_material_tensors(te, ts)
 
     def set_material_tensors(self, eps_r: torch.Tensor, sigma: torch.Tensor):
         """As set_material, from float64 device tensors of shape [n_mat][ny][nx]."""
