@@ -13,9 +13,8 @@
 //      H(k-1) is carried in registers from the previous plane;
 //   4. owned threads compute E(k) and write H(k), E(k).
 // The first plane's H(k-1) is recomputed from global memory. Ping-pong copies
-// keep every launch reading only the previous step's values. Float32 fields with
-// one component (real fields) take step3d_pair_kernel, the same schedule with two
-// x cells per thread.
+// keep every launch reading only the previous step's values. Float32 fields take
+// step3d_pair_kernel, the same schedule with two x cells per thread.
 #include "bz_internal.cuh"
 
 namespace bz {
@@ -26,7 +25,7 @@ constexpr int TX = 32;  // tile width; the tile height TY is a template paramete
 
 template <typename T>
 struct Geo3D {
-  int nx, ny, nz, pitch, n_designs, n_mat, nzb;
+  int nx, ny, nz, pitch, n_designs, n_mat, n_comp, nzb;
   long long plane, vol;  // ny*pitch, nz*plane
   T chx, chy, chz, qx, qz, inv_kd2;
 };
@@ -230,6 +229,7 @@ int launch3d(const bz_grid3d* gd, const bz_fields3d* f, int64_t step, cudaStream
   g.pitch = gd->pitch;
   g.n_designs = gd->n_designs;
   g.n_mat = gd->n_mat;
+  g.n_comp = gd->n_comp;
   g.nzb = (int)ceil_div(gd->nz, ZB);
   g.plane = (long long)gd->ny * gd->pitch;
   g.vol = g.plane * gd->nz;
@@ -254,14 +254,16 @@ int launch3d(const bz_grid3d* gd, const bz_fields3d* f, int64_t step, cudaStream
   return check_launch("bz_step3d");
 }
 
-// ---------------------------------------------------------------------------- paired columns (float32, one component)
+// ---------------------------------------------------------------------------- paired columns (float32)
 // The same step with two adjacent x cells per thread, moved as float2: a warp spans 64
 // columns whose first two (one pair, to keep 8-byte alignment) are the halo shared
 // with the neighbouring tile, so a block owns 62 x (TY-1) columns. Loads, stores,
 // shared-memory traffic, shuffles, barriers and index arithmetic are issued once per
 // pair. The pair (x, x+1) starts at an even x; when nx is odd the last pair's second
 // cell is row padding (pitch > nx), read but never stored, and no stored value
-// depends on it.
+// depends on it. Two-component (complex) fields run as two independent real fields:
+// the update is linear with real coefficients, so each block steps one component
+// (grid z = z blocks x designs x components) and reads ce and loss for it.
 __device__ __forceinline__ float2 ld2(const float* p, long long i, bool ok) {
   return ok ? __ldg(reinterpret_cast<const float2*>(p + i)) : make_float2(0.f, 0.f);
 }
@@ -280,7 +282,7 @@ struct PairIn {
 };
 
 template <int ZB, int TY>
-__global__ void __launch_bounds__(TX * TY) step3d_pair_kernel(Ptr3<float> in, Out3<float> out,
+__global__ void __launch_bounds__(TX * TY, TY == 8 ? 3 : 1) step3d_pair_kernel(Ptr3<float> in, Out3<float> out,
                                                                const float* __restrict__ ce,
                                                                const float* __restrict__ loss, Geo3D<float> g) {
   __shared__ float2 s_ez[TY][TX], s_ex[TY][TX], s_hz[TY][TX], s_hx[TY][TX];
@@ -288,8 +290,9 @@ __global__ void __launch_bounds__(TX * TY) step3d_pair_kernel(Ptr3<float> in, Ou
   const int nx = g.nx, ny = g.ny, nz = g.nz;
   const int x = blockIdx.x * (2 * TX - 2) - 2 + 2 * tx;  // first cell of the pair
   const int y = blockIdx.y * (TY - 1) - 1 + ty;
-  const int d = blockIdx.z / g.nzb;
-  const int z0 = (blockIdx.z - d * g.nzb) * ZB;
+  const int dc = blockIdx.z / g.nzb;  // design * n_comp + component
+  const int d = dc / g.n_comp;
+  const int z0 = (blockIdx.z - dc * g.nzb) * ZB;
   const int z1 = min(z0 + ZB, nz);
   const bool xin = x >= 0 && x < nx, yin = y >= 0 && y < ny, inb = xin && yin;
   const bool owned = inb && tx >= 1 && ty >= 1;
@@ -301,7 +304,7 @@ __global__ void __launch_bounds__(TX * TY) step3d_pair_kernel(Ptr3<float> in, Ou
   const long long P = g.plane;
   const long long mb = (g.n_mat > 1 ? (long long)d : 0LL) * g.vol;
   const long long col = (long long)y * g.pitch + x;
-  const long long fb = (long long)d * g.vol;
+  const long long fb = (long long)dc * g.vol;
 
   auto load_plane = [&](int k, PairIn& q) {
     const long long po = (long long)k * P + col;
@@ -423,6 +426,7 @@ int launch3d_pair(const bz_grid3d* gd, const bz_fields3d* f, int64_t step, cudaS
   g.pitch = gd->pitch;
   g.n_designs = gd->n_designs;
   g.n_mat = gd->n_mat;
+  g.n_comp = gd->n_comp;
   g.nzb = (int)ceil_div(gd->nz, ZB);
   g.plane = (long long)gd->ny * gd->pitch;
   g.vol = g.plane * gd->nz;
@@ -443,7 +447,7 @@ int launch3d_pair(const bz_grid3d* gd, const bz_fields3d* f, int64_t step, cudaS
   }
   dim3 block(TX, TY);
   dim3 grid((unsigned)ceil_div(gd->nx, 2 * TX - 2), (unsigned)ceil_div(gd->ny, TY - 1),
-            (unsigned)(g.nzb * gd->n_designs));
+            (unsigned)(g.nzb * gd->n_designs * gd->n_comp));
   step3d_pair_kernel<ZB, TY><<<grid, block, 0, st>>>(in, out, (const float*)f->ce, (const float*)f->loss, g);
   return check_launch("bz_step3d");
 }
@@ -465,7 +469,7 @@ int dispatch3d_ty(const bz_grid3d* g, const bz_fields3d* f, int64_t step, cudaSt
 
 template <typename T>
 int dispatch3d(const bz_grid3d* g, const bz_fields3d* f, int64_t step, cudaStream_t st) {
-  if (sizeof(T) == 4 && g->n_comp == 1 && pair_aligned(f)) {
+  if (sizeof(T) == 4 && pair_aligned(f) && (long long)g->n_designs * g->n_comp * ceil_div(g->nz, 8) <= 65535) {
     const bool z8 = g->tile_z == 8;
     if (g->tile_y == 16) return z8 ? launch3d_pair<8, 16>(g, f, step, st) : launch3d_pair<16, 16>(g, f, step, st);
     return z8 ? launch3d_pair<8, 8>(g, f, step, st) : launch3d_pair<16, 8>(g, f, step, st);
