@@ -187,7 +187,8 @@ __global__ void __launch_bounds__(BX) adjoint2d_kernel(AdjArgs<T> a, long long s
 // The register tile of the forward step2d_tb kernel, run backwards: a block holds 64
 // columns x NW*R rows (lane l: columns X0+l and X0+32+l) with the per-cell factors, and
 // performs TS reverse steps m = step, step-1, ..., each one the single-step adjoint
-// above: gradient from the incoming e on owned cells of the design box, U = Ce*e, the
+// above: gradient from the incoming e on owned cells of the design box (applied after
+// the last sub-step from a shared-memory history of those e), U = Ce*e, the
 // H-like pass (U(x+1) by shuffle, U(y+1) from the next row or warp), the E-like pass
 // (wx(x-1) by shuffle, wy(y-1) from the previous row or warp), carried fh*hx', fh*hy',
 // then the operations preparing step m-1 on every tile cell. Boundary rules enter the
@@ -261,25 +262,21 @@ __global__ void __launch_bounds__(32 * NW) adjoint2d_tb_kernel(AdjArgs<T> a, lon
     }
   }
 
+  // Design-box cells keep each sub-step's incoming e here ([TS][R][2][thread]); the
+  // gradient terms are applied after the last sub-step, off the barrier-paced loop.
+  extern __shared__ __align__(16) unsigned char s_hist_raw[];
+  T* s_hist = reinterpret_cast<T*>(s_hist_raw);
+  constexpr int NT = 32 * NW;
+
 #pragma unroll 1
   for (int s = 0; s < TS; ++s) {
     const long long m = step0 - s;  // reverse step taken by this sub-step
-    if (gbits) {  // grad += -e * (E_{m+1} - E_m) / eps_r on owned design-box cells
-      const long long s1 = m + 1 - a.fwd_step0;
-      if (s1 >= 1 && s1 < a.n_fwd) {
-        const long long per = (long long)a.n_designs * a.rh * a.rw;
+    if (gbits) {
 #pragma unroll
-        for (int i = 0; i < R; ++i)
+      for (int i = 0; i < R; ++i)
 #pragma unroll
-          for (int j = 0; j < 2; ++j)
-            if (gbits & (1u << (i * 2 + j))) {
-              const long long cell = (long long)(yb + i - a.ry0) * a.rw + (xs[j] - a.rx0);
-              const double en1 = (double)a.fwd[s1 * per + (long long)d * a.rh * a.rw + cell];
-              const double en0 = (double)a.fwd[(s1 - 1) * per + (long long)d * a.rh * a.rw + cell];
-              const double er = a.eps_region[(a.n_mat > 1 ? (long long)d : 0LL) * a.rh * a.rw + cell];
-              a.grad[(long long)d * a.rh * a.rw + cell] -= (double)e[i][j] * (en1 - en0) / er;
-            }
-      }
+        for (int j = 0; j < 2; ++j)
+          if (gbits & (1u << (i * 2 + j))) s_hist[((s * R + i) * 2 + j) * NT + threadIdx.x] = e[i][j];
     }
     T U[R][2];
 #pragma unroll
@@ -383,6 +380,32 @@ __global__ void __launch_bounds__(32 * NW) adjoint2d_tb_kernel(AdjArgs<T> a, lon
       if (y < ny - 1) a.hy_out[r] = hy[i][j];
     }
   }
+  // grad -= e_m * (E_{m+1} - E_m) / eps_r for each sub-step's reverse step m, in
+  // sub-step order on the owned design-box cells (no other block writes them, so the
+  // running value stays in a register between the terms)
+  if (gbits) {
+    const long long per = (long long)a.n_designs * a.rh * a.rw, db = (long long)d * a.rh * a.rw;
+    const long long eb = (a.n_mat > 1 ? (long long)d : 0LL) * a.rh * a.rw;
+#pragma unroll
+    for (int i = 0; i < R; ++i)
+#pragma unroll
+      for (int j = 0; j < 2; ++j) {
+        if (!(gbits & (1u << (i * 2 + j)))) continue;
+        const long long cell = (long long)(yb + i - a.ry0) * a.rw + (xs[j] - a.rx0);
+        const double er = a.eps_region[eb + cell];
+        double gv = a.grad[db + cell];
+#pragma unroll 1
+        for (int s = 0; s < TS; ++s) {
+          const long long s1 = step0 - s + 1 - a.fwd_step0;
+          if (s1 >= 1 && s1 < a.n_fwd) {
+            const double en1 = (double)a.fwd[s1 * per + db + cell];
+            const double en0 = (double)a.fwd[(s1 - 1) * per + db + cell];
+            gv -= (double)s_hist[((s * R + i) * 2 + j) * NT + threadIdx.x] * (en1 - en0) / er;
+          }
+        }
+        a.grad[db + cell] = gv;
+      }
+  }
 }
 
 template <typename T>
@@ -443,9 +466,17 @@ template <typename T, int TS>
 int launch_adj_tb(const bz_grid2d* g, const bz_adjoint2d* s, const bz_source_ops* ops, int64_t step, int32_t phase,
                   cudaStream_t st) {
   constexpr int R = sizeof(T) == 4 ? 4 : 2, NW = 16;
+  constexpr int hist = TS * R * 2 * 32 * NW * (int)sizeof(T);  // at most 147 KB (TS = 9)
   const AdjArgs<T> a = adj_args<T>(g, s, ops, phase);
   dim3 grid((unsigned)ceil_div(g->nx, 64 - 2 * TS), (unsigned)ceil_div(g->ny, NW * R - 2 * TS), (unsigned)g->n_designs);
-  adjoint2d_tb_kernel<T, TS, R, NW><<<grid, 32 * NW, 0, st>>>(a, (long long)step);
+  static bool opted = false;  // history plus the static tiles pass the default 48 KB
+  if (!opted) {
+    if (cudaFuncSetAttribute(adjoint2d_tb_kernel<T, TS, R, NW>, cudaFuncAttributeMaxDynamicSharedMemorySize, hist) !=
+        cudaSuccess)
+      return fail(BZ_ERR_CUDA, "bz_adjoint_step2d_multi: cannot configure the kernel's shared memory");
+    opted = true;
+  }
+  adjoint2d_tb_kernel<T, TS, R, NW><<<grid, 32 * NW, a.grad ? hist : 0, st>>>(a, (long long)step);
   return check_launch("bz_adjoint_step2d_multi");
 }
 

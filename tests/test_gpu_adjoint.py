@@ -172,3 +172,24 @@ def test_blocked_adjoint_matches_single_steps(bz, K):
     np.testing.assert_allclose(grads[0][0], grads[1][0], rtol=1e-12)
     g0, g1 = grads[0][1], grads[1][1]
     assert np.linalg.norm(g0 - g1) <= 1e-12 * np.linalg.norm(g1)
+
+
+@pytest.mark.parametrize("precision,tol", [("fp64", 1e-12), ("fp32", 1e-4)])
+@pytest.mark.parametrize("tb", [3, 5, 7, 9])
+def test_each_reverse_block_length_matches_single_steps(bz, tb, precision, tol):
+    """Reverse blocks of every length (the gradient terms of a block are applied after
+    its last sub-step) against single reverse steps, on segments of K = 100 steps that
+    no block length divides."""
+    from beamz_b200.optimization.adjoint import AdjointFDTD2D
+
+    prob, er, eps, sigma, dx, dt, n_steps, src, mon, mode, f0, region = _problem(bz, B=2, K=100, seed=4)
+    freqs = [0.97 * f0, f0]
+    grads = []
+    for blk in (tb, 1):
+        p = AdjointFDTD2D(eps, sigma, dx, dt, n_steps, [src], mon, np.stack([mode, mode]), freqs, region,
+                          n_designs=2, precision=precision, checkpoint_every=100)
+        p.forward(er)
+        p._adj_block = blk
+        grads.append(p.backward())
+    assert np.abs(grads[0]).max() > 0
+    assert np.linalg.norm(grads[0] - grads[1]) <= tol * np.linalg.norm(grads[1])
