@@ -392,17 +392,17 @@ __global__ void __launch_bounds__(32 * NW) adjoint2d_tb_kernel(AdjArgs<T> a, lon
       for (int j = 0; j < 2; ++j) {
         if (!(gbits & (1u << (i * 2 + j)))) continue;
         const long long cell = (long long)(yb + i - a.ry0) * a.rw + (xs[j] - a.rx0);
+        const long long p0 = step0 + 1 - a.fwd_step0;  // captured plane E_{m+1} of sub-step 0
+        T f[TS + 1];  // planes p0, p0-1, ..., p0-TS, all loads issued before the sums
+#pragma unroll
+        for (int k = 0; k <= TS; ++k)
+          f[k] = (p0 - k >= 0 && p0 - k < a.n_fwd) ? a.fwd[(p0 - k) * per + db + cell] : T(0);
         const double er = a.eps_region[eb + cell];
         double gv = a.grad[db + cell];
-#pragma unroll 1
-        for (int s = 0; s < TS; ++s) {
-          const long long s1 = step0 - s + 1 - a.fwd_step0;
-          if (s1 >= 1 && s1 < a.n_fwd) {
-            const double en1 = (double)a.fwd[s1 * per + db + cell];
-            const double en0 = (double)a.fwd[(s1 - 1) * per + db + cell];
-            gv -= (double)s_hist[((s * R + i) * 2 + j) * NT + threadIdx.x] * (en1 - en0) / er;
-          }
-        }
+#pragma unroll
+        for (int s = 0; s < TS; ++s)
+          if (p0 - s >= 1 && p0 - s < a.n_fwd)
+            gv -= (double)s_hist[((s * R + i) * 2 + j) * NT + threadIdx.x] * ((double)f[s] - (double)f[s + 1]) / er;
         a.grad[db + cell] = gv;
       }
   }
