@@ -11,7 +11,7 @@ from oracle import fdtd2d
 pytestmark = pytest.mark.gpu
 
 
-def _problem(bz, B=1, precision="fp64", n_steps=360, K=128, seed=0):
+def _problem(bz, B=1, precision="fp64", n_steps=360, K=128, seed=0, store_history="auto"):
     from beamz_b200.optimization.adjoint import AdjointFDTD2D
 
     ny, nx, dx = 48, 64, 20e-9
@@ -32,16 +32,17 @@ def _problem(bz, B=1, precision="fp64", n_steps=360, K=128, seed=0):
     mode = np.exp(-(y / 4.0) ** 2).astype(complex)
     region = (16, 24, 16, 14)
     prob = AdjointFDTD2D(eps, sigma, dx, dt, n_steps, [src], mon, mode, f0, region, n_designs=B,
-                         precision=precision, checkpoint_every=K)
+                         precision=precision, checkpoint_every=K, store_history=store_history)
     rng = np.random.default_rng(seed)
     er = 2.085 + 10.165 * rng.random((B, region[2], region[3]))
     return prob, er, eps, sigma, dx, dt, n_steps, src, mon, mode, f0, region
 
 
 # K = 100 leaves single steps between graph chunks at every checkpoint
+@pytest.mark.parametrize("store_history", [False, True])
 @pytest.mark.parametrize("K", [128, 100])
-def test_adjoint_matches_central_differences_fp64(bz, K):
-    prob, er, *_ = _problem(bz, K=K)
+def test_adjoint_matches_central_differences_fp64(bz, K, store_history):
+    prob, er, *_ = _problem(bz, K=K, store_history=store_history)
     J, g = prob.value_and_grad(er)
     rng = np.random.default_rng(99)
     h = 1e-3
@@ -174,9 +175,10 @@ def test_blocked_adjoint_matches_single_steps(bz, K):
     assert np.linalg.norm(g0 - g1) <= 1e-12 * np.linalg.norm(g1)
 
 
+@pytest.mark.parametrize("store_history", [False, True])
 @pytest.mark.parametrize("precision,tol", [("fp64", 1e-12), ("fp32", 1e-4)])
 @pytest.mark.parametrize("tb", [3, 5, 7, 9])
-def test_each_reverse_block_length_matches_single_steps(bz, tb, precision, tol):
+def test_each_reverse_block_length_matches_single_steps(bz, tb, precision, tol, store_history):
     """Reverse blocks of every length (the gradient terms of a block are applied after
     its last sub-step) against single reverse steps, on segments of K = 100 steps that
     no block length divides."""
@@ -187,9 +189,30 @@ def test_each_reverse_block_length_matches_single_steps(bz, tb, precision, tol):
     grads = []
     for blk in (tb, 1):
         p = AdjointFDTD2D(eps, sigma, dx, dt, n_steps, [src], mon, np.stack([mode, mode]), freqs, region,
-                          n_designs=2, precision=precision, checkpoint_every=100)
+                          n_designs=2, precision=precision, checkpoint_every=100, store_history=store_history)
         p.forward(er)
         p._adj_block = blk
         grads.append(p.backward())
     assert np.abs(grads[0]).max() > 0
     assert np.linalg.norm(grads[0] - grads[1]) <= tol * np.linalg.norm(grads[1])
+
+
+@pytest.mark.parametrize("precision,tol", [("fp64", 1e-12), ("fp32", 1e-5)])
+def test_forward_history_equals_checkpoint_recompute(bz, precision, tol):
+    """The gradient from the region history kept during the forward run equals the one
+    from checkpoints and segment recomputes (same forward values, same reverse steps)."""
+    out = []
+    for store in (True, False):
+        prob, er, *_ = _problem(bz, B=3, precision=precision, K=100, seed=7, store_history=store)
+        J, g = prob.value_and_grad(er)
+        assert prob._hist_ready == store and (prob._hist is not None) == store
+        out.append((J, g))
+    np.testing.assert_allclose(out[0][0], out[1][0], rtol=1e-13)
+    assert np.linalg.norm(out[0][1] - out[1][1]) <= tol * np.linalg.norm(out[1][1])
+
+
+def test_backward_without_checkpoints_or_history_is_an_error(bz):
+    prob, er, *_ = _problem(bz, K=100, store_history=True)
+    prob.forward(er, keep_checkpoints=False)
+    with pytest.raises(RuntimeError):
+        prob.backward()
