@@ -380,9 +380,8 @@ __global__ void __launch_bounds__(32 * NW) adjoint2d_tb_kernel(AdjArgs<T> a, lon
       if (y < ny - 1) a.hy_out[r] = hy[i][j];
     }
   }
-  // grad -= e_m * (E_{m+1} - E_m) / eps_r for each sub-step's reverse step m, in
-  // sub-step order on the owned design-box cells (no other block writes them, so the
-  // running value stays in a register between the terms)
+  // grad -= sum over the sub-steps' reverse steps m of e_m * (E_{m+1} - E_m), over
+  // eps_r, on the owned design-box cells (no other block writes them)
   if (gbits) {
     const long long per = (long long)a.n_designs * a.rh * a.rw, db = (long long)d * a.rh * a.rw;
     const long long eb = (a.n_mat > 1 ? (long long)d : 0LL) * a.rh * a.rw;
@@ -398,12 +397,13 @@ __global__ void __launch_bounds__(32 * NW) adjoint2d_tb_kernel(AdjArgs<T> a, lon
         for (int k = 0; k <= TS; ++k)
           f[k] = (p0 - k >= 0 && p0 - k < a.n_fwd) ? a.fwd[(p0 - k) * per + db + cell] : T(0);
         const double er = a.eps_region[eb + cell];
-        double gv = a.grad[db + cell];
+        const double gv = a.grad[db + cell];
+        T acc = T(0);  // the block's terms in the fields' precision (e and the planes are T)
 #pragma unroll
         for (int s = 0; s < TS; ++s)
           if (p0 - s >= 1 && p0 - s < a.n_fwd)
-            gv -= (double)s_hist[((s * R + i) * 2 + j) * NT + threadIdx.x] * ((double)f[s] - (double)f[s + 1]) / er;
-        a.grad[db + cell] = gv;
+            acc += s_hist[((s * R + i) * 2 + j) * NT + threadIdx.x] * (f[s] - f[s + 1]);
+        a.grad[db + cell] = gv - (double)acc / er;
       }
   }
 }
