@@ -181,3 +181,29 @@ def test_time_accumulation_matches_repeated_addition():
         t_loop += dt
     t_acc = float(np.add.accumulate(np.r_[1.0e-15, np.full(20000, dt)])[-1])
     assert t_acc == t_loop
+
+
+def test_adjoint_history_auto_takes_at_most_half_the_free_memory(monkeypatch):
+    """store_history="auto" keeps the forward region history when (n_steps + 1) x designs x
+    region cells fit in half the free device memory (a faked memory query; no GPU)."""
+    import types
+
+    import torch
+
+    from beamz_b200.optimization.adjoint import AdjointFDTD2D
+
+    p = AdjointFDTD2D.__new__(AdjointFDTD2D)
+    p.store_history, p._hist, p.region, p.n_steps, p.B = "auto", None, (0, 0, 120, 120), 8000, 64
+    p.engine = types.SimpleNamespace(dtype=torch.float32, dev=None)
+    need = 8001 * 64 * 120 * 120 * 4  # 29.5 GB
+    monkeypatch.setattr(torch.cuda, "mem_get_info", lambda dev=None: (2 * need, 4 * need))
+    assert p._use_history()
+    monkeypatch.setattr(torch.cuda, "mem_get_info", lambda dev=None: (2 * need - 2, 4 * need))
+    assert not p._use_history()
+    p._hist = object()  # once allocated, it is kept
+    assert p._use_history()
+    p._hist = None
+    p.store_history = False
+    assert not p._use_history()
+    p.store_history = True
+    assert p._use_history()
