@@ -271,7 +271,15 @@ def rasterize_2d(design, cs: float, gw: int, gh: int):
     nat.rasterize2d(gw, gh, _ptr(t_x), _ptr(t_y), _ptr(t_off), _ptr(t_cor), _ptr(t_bg), _ptr(t_shapes), len(shapes),
                     _ptr(t_paths), _ptr(t_verts), _ptr(t_custom), _ptr(t_pml), len(pmls), _ptr(t_tab), float(cs),
                     EPS_0, MU_0, eps.data_ptr(), mu.data_ptr(), sig.data_ptr(), stream)
-    return eps.cpu().numpy(), mu.cpu().numpy(), sig.cpu().numpy()
+    return to_host(eps), to_host(mu), to_host(sig)
+
+
+def to_host(t: torch.Tensor) -> np.ndarray:
+    """A device grid as a NumPy array in page-locked host memory (the array keeps the
+    pinned buffer alive), so that a simulation's upload of it runs at full copy speed."""
+    h = torch.empty(t.shape, dtype=t.dtype, pin_memory=True)
+    h.copy_(t)
+    return h.numpy()
 
 
 class RegularGrid(BaseMeshGrid):

@@ -19,7 +19,7 @@ import torch
 from .. import _native as nat
 from ..const import EPS_0, MU_0
 from ..design.materials import material_triple
-from .meshing import BaseMeshGrid, _compile_pml, _dev_struct_array, _device, _ptr
+from .meshing import BaseMeshGrid, _compile_pml, _dev_struct_array, _device, _ptr, to_host
 
 
 def _resolutions(design, resolution_xy, resolution_z):
@@ -135,7 +135,7 @@ def init_regular_grid_3d(grid, design, resolution_xy=None, resolution_z=None, ex
                     _ptr(t_zw), _ptr(t_paths), _ptr(t_verts), _ptr(t_pml), len(pmls), _ptr(t_tab), _ptr(t_pz), sf_z,
                     float(rxy), EPS_0, MU_0, eps.data_ptr(), mu.data_ptr(), sig.data_ptr(),
                     torch.cuda.current_stream().cuda_stream)
-    grid.permittivity, grid.permeability, grid.conductivity = eps.cpu().numpy(), mu.cpu().numpy(), sig.cpu().numpy()
+    grid.permittivity, grid.permeability, grid.conductivity = to_host(eps), to_host(mu), to_host(sig)
     grid.shape = grid.permittivity.shape
     grid.dx, grid.dy, grid.dz = rxy, rxy, rz
     grid.extrude = extrude
