@@ -1,5 +1,5 @@
 """The oracle reproduces the reference's own outputs (golden fixtures from
-tests/golden/make_golden.py) — this pins the checker before it judges the GPU."""
+tests/golden/make_golden.py) — this pins the oracle before the GPU path is compared with it."""
 import numpy as np
 import pytest
 
