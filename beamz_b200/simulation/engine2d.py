@@ -72,6 +72,7 @@ class Engine2D:
         self.d_step = torch.zeros(1, dtype=torch.int64, device=self.dev)
         self.use_graphs = use_graphs
         self._graphs: dict[int, torch.cuda.CUDAGraph] = {}
+        self.kernel_timer = None  # graphs.KernelTimer around the step launches (direct launches only)
         self._autotune = time_block == "auto"
         if self._autotune:
             time_block = 7
@@ -206,13 +207,23 @@ class Engine2D:
         return self.step_index & 1
 
     def _launch(self, step_arg: int, d_step_ptr):
+        timer = self.kernel_timer
+        if timer is not None:
+            timer.before()
         nat.step2d(self.grid, self._fields(), self.sops if self.sops.n_ops else None,
                    self.mops if self.mops.n_points else None, step_arg, d_step_ptr, self._stream())
+        if timer is not None:
+            timer.after()
 
     def _launch_tb(self, step_arg: int, d_step_ptr):
+        timer = self.kernel_timer
+        if timer is not None:
+            timer.before()
         nat.step2d_multi(self.grid, self._fields(), self.sops if self.sops.n_ops else None,
                          self.mops if self.mops.n_points else None, step_arg, self.time_block, self.tb_tile,
                          d_step_ptr, self._stream())
+        if timer is not None:
+            timer.after()
 
     def _block(self) -> int:
         """Steps per launch available now."""
@@ -322,7 +333,7 @@ class Engine2D:
             if self.record is not None:
                 room = min(room, self.mops.rec_step0 + self.rec_rows - self.step_index)
             tb = self._block()
-            if self.use_graphs and not self.mops.region and room >= self.chunk:
+            if self.use_graphs and self.kernel_timer is None and not self.mops.region and room >= self.chunk:
                 # the chunk writes `chunk` ring slots: fold what earlier launches left
                 # there first, or those samples are overwritten before they are read
                 if self.step_index - self._folded > RING_LEN - self.chunk:

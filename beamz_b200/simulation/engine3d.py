@@ -80,6 +80,7 @@ class Engine3D:
         self.d_step = torch.zeros(1, dtype=torch.int64, device=self.dev)
         self.use_graphs = use_graphs
         self._graphs = {}
+        self.kernel_timer = None  # graphs.KernelTimer around the step launches (direct launches only)
         # kernels per step: the step itself, source operations, monitor gather, power
         self.kernels_per_step = 1 + (self.sops.n_ops > 0) + (self.gops is not None) + (self.power is not None)
         self.n_step_launches = 0  # bz_step3d launches (one per step, graph nodes included)
@@ -179,7 +180,12 @@ class Engine3D:
     def _launch(self, step_arg, d_step_ptr):
         st = self._stream()
         fields = self._fields()
+        timer = self.kernel_timer
+        if timer is not None:
+            timer.before()
         nat.step3d(self.grid, fields, step_arg, st)
+        if timer is not None:
+            timer.after()
         dst = (step_arg & 1) ^ 1
         if self.sops.n_ops:
             nat.cell_ops(self.f["Ez"][dst].data_ptr(), self.bz_dtype, self.n_designs, self.n_comp, self.vol, self.nx,
@@ -217,7 +223,7 @@ class Engine3D:
             room = n
             if self.record is not None:
                 room = min(room, self.gops.rec_step0 + self.rec_rows - self.step_index)
-            if self.use_graphs and room >= GRAPH_CHUNK:
+            if self.use_graphs and self.kernel_timer is None and room >= GRAPH_CHUNK:
                 # fold samples left by single steps before the chunk overwrites their slots
                 if self.step_index - self._folded > RING_LEN - GRAPH_CHUNK:
                     self._fold()

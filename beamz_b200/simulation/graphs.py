@@ -28,6 +28,41 @@ def capture(launches) -> torch.cuda.CUDAGraph:
     return g
 
 
+class KernelTimer:
+    """CUDA-event timing of an engine's step-kernel launches, for direct (non-graph)
+    launches: the engine calls ``before()``/``after()`` around each step-kernel launch
+    on the launching stream; every ``every``-th launch is bracketed by an event pair.
+    Events recorded during a graph capture cannot be timed, so engines run without
+    graphs while a timer is attached."""
+
+    def __init__(self, every: int = 1, capacity: int = 4096):
+        self.every = max(1, int(every))
+        self.pairs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+                      for _ in range(capacity)]
+        self.n_launch = 0
+        self.used = 0
+        self._open = False
+
+    def before(self):
+        self._open = self.n_launch % self.every == 0 and self.used < len(self.pairs)
+        if self._open:
+            self.pairs[self.used][0].record()
+
+    def after(self):
+        if self._open:
+            self.pairs[self.used][1].record()
+            self.used += 1
+        self._open = False
+        self.n_launch += 1
+
+    def durations_ms(self):
+        """Durations of the timed launches (synchronizes on the last one)."""
+        if self.used == 0:
+            return []
+        self.pairs[self.used - 1][1].synchronize()
+        return [a.elapsed_time(b) for a, b in self.pairs[:self.used]]
+
+
 def dft_phasors(freqs, n_steps: int, dt: float, device) -> torch.Tensor:
     """[n_steps][n_freq][4] float64 table (cos wt_E, -sin wt_E, cos wt_H, -sin wt_H) with
     t_E = (n+1) dt and t_H = (n+1/2) dt, computed on the device (the angles are the

@@ -45,7 +45,7 @@ def parse():
     p.add_argument("--steps", type=int, default=5)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    p.add_argument("--workload", default="mmi_2d",
+    p.add_argument("--workload", default="soi_mmi_3d",
                    choices=["mmi_2d", "dipole_2d", "soi_mmi_3d", "topo_2d", "surrogate_2d"])
     p.add_argument("--samples", type=int, default=20000, help="surrogate_2d: FDTD-labelled training samples")
     p.add_argument("--epochs", type=int, default=20, help="surrogate_2d: training epochs")
@@ -59,6 +59,13 @@ def parse():
     return p.parse_args()
 
 
+DESC = {"mmi_2d": "2D TE 1x2 MMI splitter, 2000x1000 cells at 20 nm, 30-cell PML, CW mode source, "
+                  "5-wavelength DFT flux monitors",
+        "dipole_2d": "2D point dipole in vacuum, 400x400 cells at 20 nm, 20-cell PML, 4 edge monitors",
+        "soi_mmi_3d": "3D SOI strip into a 6x3 um MMI, 600x300x150 cells at 20 nm, 16-cell PML on all faces, "
+                      "Gaussian-pulse mode source, 5-wavelength DFT flux planes on both outputs"}
+
+
 def workload(name, n_steps=None, nz=None):
     from beamz_b200 import workloads as W
 
@@ -66,14 +73,21 @@ def workload(name, n_steps=None, nz=None):
     if nz is not None and name == "soi_mmi_3d":
         kw["nz"] = nz  # thinner 3D grid (profiling cases)
     d, t, dx = getattr(W, name)(**kw)
-    desc = {"mmi_2d": "2D TE 1x2 MMI splitter, 2000x1000 cells at 20 nm, 30-cell PML, CW mode source, "
-                      "5-wavelength DFT flux monitors",
-            "dipole_2d": "2D point dipole in vacuum, 400x400 cells at 20 nm, 20-cell PML, 4 edge monitors",
-            "soi_mmi_3d": "3D SOI strip into a 6x3 um MMI, 600x300x150 cells at 20 nm, 16-cell PML on all faces, "
-                          "Gaussian-pulse mode source, 5-wavelength DFT flux planes on both outputs"}[name]
+    desc = DESC[name]
     if nz is not None and name == "soi_mmi_3d":
         desc += f" (here {nz} z planes)"
     return d, t, dx, desc
+
+
+def _config(name, shape, n_steps, world):
+    """The workload's config, identical in both arms: what is stepped, not how."""
+    cells = int(np.prod(shape))
+    is3d = len(shape) == 3
+    state = cells * ((6 * 4 * 2 + 8) if is3d else (3 * 4 * 2 + 8))  # fp32 fields (two copies) + coefficients
+    l2 = (f"inputs larger than L2: {state / 1e6:.0f} MB of fields and coefficients against 126 MB"
+          if state > 126e6 else "device L2 flushed (512 MB write) before every run")
+    return {"workload": DESC[name] if len(shape) != 3 or shape[0] == 150 else DESC[name] + f" ({shape[0]} z planes)",
+            "grid": [int(v) for v in shape], "time_steps": int(n_steps), "l2": l2, "parallelism": f"replicas x{world}"}
 
 
 def max_over_ranks(ms: float, world: int, device="cpu") -> float:
@@ -144,18 +158,34 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
-def profiled_traffic(kernel="step2d", workload_name="mmi_2d"):
-    """dram bytes per launch from the committed ncu summary, if present."""
+def profiled_traffic(kernel, workload_name):
+    """DRAM bytes per launch of `kernel` from the committed ncu summary
+    profiles/<kernel>_<workload>.txt, used only while the kernel source it was captured
+    on is unchanged (the summary records the SHA-256 of that .cu file)."""
+    import hashlib
+
     p = ROOT / "profiles" / f"{kernel}_{workload_name}.txt"
     if not p.exists():
-        return None
+        return None, "not profiled"
+    val = src = sha = None
     for line in p.read_text().splitlines():
         if line.startswith("traffic_bytes_per_launch:"):
             try:
-                return float(line.split(":", 1)[1])
+                val = float(line.split(":", 1)[1])
             except ValueError:
-                return None
-    return None
+                val = None
+        elif line.startswith("source_sha256:"):
+            parts = line.split(":", 1)[1].split()
+            if len(parts) == 2:
+                src, sha = parts
+    if val is None:
+        return None, "not in the profile summary"
+    if not src or not (ROOT / src).exists():
+        return None, "profile summary names no source file"
+    now = hashlib.sha256((ROOT / src).read_bytes()).hexdigest()
+    if now != sha:
+        return None, f"stale: {src} changed since the ncu capture"
+    return val, f"from one ncu capture (profiles/{p.name}) of the current {src}"
 
 
 def cpu_baseline(d, t, dx, n_steps):
@@ -179,6 +209,8 @@ def run_b200(args):
     import torch
     import torch.distributed as dist
 
+    from beamz_b200.simulation.graphs import KernelTimer
+
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -199,10 +231,12 @@ def run_b200(args):
     sim.initialize_simulation(save=False, live=False, save_memory_mode=True)
     eng = sim.engine
     flush = torch.empty(512 << 20, dtype=torch.uint8, device="cuda")
+    flush_l2 = cells * (56 if is3d else 32) <= 126e6  # inputs smaller than L2: flush it before every run
 
     def one_run(evs=None):
         eng.reset()
-        flush.fill_(1)
+        if flush_l2:
+            flush.fill_(1)
         if evs is not None:
             evs[0].record()
         eng.run_steps(n_steps)
@@ -211,12 +245,18 @@ def run_b200(args):
 
     count = (lambda: eng.n_kernel_launches) if is3d else (lambda: eng.n_step_launches + eng.n_fold_launches)
     l0, k0 = eng.n_step_launches, count()
-    one_run()
+    one_run()  # the 2D engine picks its launch shape here (autotuner)
     step_launches, all_launches = eng.n_step_launches - l0, count() - k0
 
+    # Timed runs use direct launches with CUDA events around the step kernel (events in a
+    # captured graph cannot be timed); every `every`-th step launch is bracketed.
+    every = max(1, step_launches * (args.steps + args.warmup) // 4000)
     for _ in range(args.warmup):
+        eng.kernel_timer = KernelTimer(every=every, capacity=8)
         one_run()
     torch.cuda.synchronize()
+    timer = KernelTimer(every=every, capacity=step_launches * args.steps // every + 8)
+    eng.kernel_timer = timer
     gpu_id = "GPU-" + str(torch.cuda.get_device_properties(local).uuid)
     clocks = ClockSampler(gpu_id)
     clocks.start()
@@ -234,21 +274,22 @@ def run_b200(args):
     if world > 1:
         dist.barrier()
     ck = clocks.stop()
+    eng.kernel_timer = None
     total_ms = t_start.elapsed_time(t_end)
-    run_ms = [a.elapsed_time(b) for a, b in evs]
+    kern_ms = timer.durations_ms()
     total_ms = max_over_ranks(total_ms, world, "cuda")
     value = world * args.steps * cells * n_steps / (total_ms * 1e-3) / 1e9
 
-    # dominant kernel: the time-blocked 2D step launch (time_block steps per launch) or the
-    # 3D step launch (one step); the run time also holds the small monitor/source/fold
-    # launches (about 1 % in 2D by the ncu launch list)
-    tb = getattr(eng, "time_block", 1)
-    per_launch_s = sum(run_ms) * 1e-3 / (args.steps * step_launches)
+    # dominant kernel: the 3D step (one step per launch) or the time-blocked 2D step
+    # (time_block steps per launch); algorithmic bytes per launch over its mean duration
+    tb = getattr(eng, "time_block", 1) if not is3d else 1
     cell_bytes = (48 * args.n_comp + 8) if is3d else (24 * args.n_comp + 8)
-    algo_bytes = cell_bytes * cells * n_steps / step_launches  # per launch: steps x B/cell x cells
+    algo_bytes = cell_bytes * cells * tb  # per launch: steps x B/cell x cells
     peak, peak_kind = measured_peaks()
-    achieved = algo_bytes / per_launch_s / 1e9
-    traffic = profiled_traffic("step3d" if is3d else "step2d_tb", args.workload)
+    kernel_s = float(np.mean(kern_ms)) * 1e-3
+    achieved = algo_bytes / kernel_s / 1e9
+    kname = "step3d" if is3d else "step2d_tb"
+    traffic, traffic_note = profiled_traffic(kname, args.workload)
 
     e2e = None
     if not args.no_e2e:
@@ -261,14 +302,17 @@ def run_b200(args):
         v, el = cpu_baseline(d, t, dx, ncpu)
         cpu = {"value": v, "unit": UNIT, "cores": 1, "kind": "port",
                "sample": f"first {ncpu} of {n_steps} time steps of the same workload, float64 NumPy "
-                         f"(the reference's NumPy backend and step helpers restated in oracle/), {el:.1f} s"}
+                         f"(the reference's NumPy stepping loop restated in oracle/), {el:.1f} s"}
     flux = None
     try:
         sim2 = e2e.pop("_sim") if e2e else None
-        if sim2 is not None:
+        if sim2 is not None and not is3d:
             tin = next(m for m in sim2.monitors if m.name == "in").flux()
             tp = [next(m for m in sim2.monitors if m.name == n).flux() for n in ("port_top", "port_bottom")]
             flux = {"T_top": list(np.round(tp[0] / tin, 4)), "T_bottom": list(np.round(tp[1] / tin, 4))}
+        elif sim2 is not None:
+            flux = {n: [float(f"{v:.4g}") for v in next(m for m in sim2.monitors if m.name == n).flux()]
+                    for n in ("port_top", "port_bottom")}
     except Exception:  # noqa: BLE001 - the transmission readout is informational only
         flux = None
     if rank == 0:
@@ -276,8 +320,8 @@ def run_b200(args):
             "metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(total_ms / args.steps, 3), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": desc, "grid": list(shape), "time_steps": n_steps, "step": "one full run",
-                       "l2": "flushed (512 MB write) before every run", "parallelism": f"replicas x{world}"},
+            "config": _config(args.workload, shape, n_steps, world),
+            "bench_step": f"one full run of {n_steps} time steps from zero fields (direct launches)",
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                          "frac": round(achieved / peak, 4), "traffic": traffic},
             "cpu_baseline": cpu,
@@ -285,20 +329,26 @@ def run_b200(args):
             "gpu_launches": args.steps * all_launches,
             "clocks": ck,
         }
+        timing = (f"mean of {len(kern_ms)} {kname} launches timed with CUDA events inside the timed runs "
+                  f"(every {every}-th launch), {kernel_s * 1e6:.1f} us each; the runs' other kernels (sources, "
+                  f"monitor samples, DFT folds) take {100 * (1 - kernel_s * step_launches / (total_ms / args.steps * 1e-3)):.1f} % "
+                  f"of the run")
         if is3d:
-            line["config"]["tile"] = "32 x 8 columns x 16 planes"
-            line["roofline"]["note"] = (f"step3d: one step per launch x {cell_bytes} B/cell (six fields read and "
-                                        f"written, ce and loss read) x {cells} cells; peak {peak_kind}")
+            line["roofline"]["note"] = (f"{kname}: one time step per launch x {cell_bytes} B/cell (six fields read "
+                                        f"and written, ce and loss read) x {cells} cells; {timing}; peak "
+                                        f"{peak_kind} copy bandwidth; traffic {traffic_note}")
+            line["tile"] = "paired columns: 32 x 8 threads x 2 cells, 16-plane z blocks"
         else:
-            line["config"].update(time_block=tb, tb_tile=eng.tb_tile, tile_choice="autotuned",
-                                  tune_us_per_step={f"{k[0]}/{k[1]}": round(v * 1e3, 3)
-                                                    for k, v in getattr(eng, "tune_times", {}).items()})
-            line["roofline"]["note"] = (f"step2d_tb: {tb} steps per launch x {cell_bytes} B/cell (algorithmic, "
-                                        f"one-step) x {cells} cells; peak {peak_kind}; temporal blocking keeps the "
-                                        f"tile on chip between sub-steps, so DRAM traffic per launch is one read "
-                                        f"of the inputs and one write of the owned cells")
+            line["roofline"]["note"] = (f"{kname}: {tb} time steps per launch x {cell_bytes} B/cell (algorithmic, "
+                                        f"one-step) x {cells} cells; {timing}; peak {peak_kind} copy bandwidth; "
+                                        f"temporal blocking keeps the tile on chip between sub-steps, so DRAM traffic "
+                                        f"per launch is one read of the inputs and one write of the owned cells; "
+                                        f"traffic {traffic_note}")
+            line["tuning"] = {"time_block": tb, "tb_tile": eng.tb_tile, "tile_choice": "autotuned",
+                              "tune_us_per_step": {f"{k[0]}/{k[1]}": round(v * 1e3, 3)
+                                                   for k, v in getattr(eng, "tune_times", {}).items()}}
         if flux:
-            line["transmission"] = flux
+            line["transmission" if not is3d else "port_flux"] = flux
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.barrier()
@@ -331,26 +381,112 @@ def run_e2e(grid, t, cells, n_steps, args, world):
 
 
 # ---------------------------------------------------------------------------- reference arm
+REF_DIR = ROOT / "baseline" / "_ref"
+_STUBBED = ["matplotlib", "matplotlib.pyplot", "matplotlib.patches", "matplotlib.path", "matplotlib.animation",
+            "mpl_toolkits", "mpl_toolkits.mplot3d", "gdspy"]
+
+
+def reference_api():
+    """The reference package from baseline/_ref, imported with stand-ins for its plotting
+    and GDS imports (matplotlib, mpl_toolkits and gdspy are absent here and are not on the
+    stepping path), as a namespace of its public names plus gaussian_pulse, RegularGrid3D,
+    BaseMeshGrid and FDTD. Nothing of beamz_b200 is imported."""
+    import types
+    from unittest.mock import MagicMock
+
+    if not (REF_DIR / "beamz" / "simulation" / "fdtd.py").exists():
+        raise FileNotFoundError(f"the reference is not installed under {REF_DIR}")
+    for m in _STUBBED:
+        sys.modules.setdefault(m, MagicMock())
+    if str(REF_DIR) not in sys.path:
+        sys.path.insert(0, str(REF_DIR))
+    import beamz
+    from beamz.devices import signals
+    from beamz.simulation import meshing
+    from beamz.simulation.fdtd import FDTD
+
+    ns = {k: getattr(beamz, k) for k in dir(beamz) if not k.startswith("_")}
+    ns.update(gaussian_pulse=signals.gaussian_pulse, RegularGrid3D=meshing.RegularGrid3D,
+              BaseMeshGrid=meshing.BaseMeshGrid, FDTD=FDTD)
+    return types.SimpleNamespace(**ns)
+
+
+def workload_module():
+    """beamz_b200/workloads.py loaded by path: its builders take the API namespace as an
+    argument and import nothing of the package at module level."""
+    import importlib.util
+
+    spec = importlib.util.spec_from_file_location("bz_workload_defs", ROOT / "beamz_b200" / "workloads.py")
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def _quiet_child():
+    """Route a worker's stdout (the reference prints rich status lines) to stderr, so the
+    arm's JSON line is the only thing on stdout."""
+    os.dup2(2, 1)
+    sys.stdout = sys.stderr
+
+
 def run_reference(args):
+    """The reference's own CPU path (the reference package, its NumPy backend and step
+    helpers) on the host cores, for the same workload and config as the b200 arm.
+
+    2D: one copy of the whole workload per host core (NumPy runs one core per process),
+    each advancing `sample` time steps per bench step through FDTD.step(); value = all
+    copies' cell updates over the slowest copy's time.
+
+    3D: the workload's grid does not fit one process per core (the reference's step holds
+    about 600 B per cell, 17 GB on 600 x 300 x 150), so the grid is split into P z-slabs,
+    each stepped by the reference's FDTD in its own process with its slab's material and
+    the source points that fall in it (slabs exchange nothing: the partition changes no
+    per-cell work, only the values at slab faces); one bench step = one time step of
+    every slab, i.e. one time step of the whole grid; value = grid cells x steps over the
+    slowest slab's time. The x-normal plane monitors are left out: the reference's
+    x-normal monitor indexes the wrong coordinate and fails (monitors.py:222-273)."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    d, t, dx, desc = workload(args.workload, args.time_steps)
-    if d.is_3d and d.depth:
-        print(json.dumps({"impl": "reference", "unavailable": "the 3-D material grid is rasterised on the GPU "
-                          "only; the b200 line's cpu_baseline times the 3-D CPU loop on two steps"}), flush=True)
+    try:
+        api = reference_api()
+    except Exception as e:  # noqa: BLE001
+        print(json.dumps({"impl": "reference", "unavailable": f"reference package not importable: {e}"}),
+              flush=True)
         return
+    Wm = workload_module()
+    kw = {} if args.time_steps is None else {"n_steps": args.time_steps}
+    is3d = args.workload == "soi_mmi_3d"
+    d, t, dx = getattr(Wm, args.workload)(api=api, monitors=not is3d, **kw)
     import multiprocessing as mp
 
-    # NumPy steps one grid on one core, so the reference uses the host's cores as
-    # independent copies of the same sample (spawned: the parent holds no GPU state).
-    n_proc = max(1, min(64, len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()))
+    ncore = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()
     for var in ("OMP_NUM_THREADS", "OPENBLAS_NUM_THREADS", "MKL_NUM_THREADS"):
-        os.environ.setdefault(var, "1")  # one thread per copy (the mode solver's BLAS too)
+        os.environ.setdefault(var, "1")  # one thread per process (the mode solver's BLAS too)
     ctx = mp.get_context("spawn")
+    tmp = None
+    if is3d:
+        from oracle import raster3d
+
+        eps, _, sig = raster3d.rasterize3d(d, dx, extrude=True)
+        shape = list(eps.shape)
+        nz = eps.shape[0]
+        n_proc = max(1, min(64, ncore, nz // 4))
+        edges = np.linspace(0, nz, n_proc + 1).round().astype(int)
+        tmp = tempfile.mkdtemp(prefix="bz_ref3d_")
+        np.save(os.path.join(tmp, "eps.npy"), eps)
+        np.save(os.path.join(tmp, "sig.npy"), sig)
+        del eps, sig
+        jobs = [("3d", (int(edges[k]), int(edges[k + 1])), tmp) for k in range(n_proc)]
+        sample = 1
+    else:
+        shape = None
+        n_proc = max(1, min(64, ncore))
+        jobs = [("2d", None, None)] * n_proc
+        sample = max(1, min(10, len(t)))
     barrier, q = ctx.Barrier(n_proc, timeout=1800), ctx.Queue()
-    procs = [ctx.Process(target=_reference_worker, args=(args.workload, args.time_steps, args.steps, args.warmup,
-                                                          barrier, q)) for _ in range(n_proc)]
+    procs = [ctx.Process(target=_reference_worker, args=(args.workload, args.time_steps, job, sample, args.steps,
+                                                          args.warmup, barrier, q)) for job in jobs]
     for pr in procs:
         pr.start()
     res = []
@@ -362,54 +498,103 @@ def run_reference(args):
             pr.join(timeout=60)
             if pr.is_alive():
                 pr.terminate()
-    if any(r is None for r in res):
-        print(json.dumps({"impl": "reference", "unavailable": "a reference worker failed"}), flush=True)
+        if tmp:
+            import shutil
+
+            shutil.rmtree(tmp, ignore_errors=True)
+    bad = [r for r in res if not isinstance(r, tuple)]
+    if bad:
+        print(json.dumps({"impl": "reference", "unavailable": f"a reference worker failed: {bad[0]}"}), flush=True)
         return
     el = max(r[0] for r in res)
-    cells, sample, shape = res[0][1], res[0][2], res[0][3]
-    value = n_proc * args.steps * cells * sample / el / 1e9
+    if is3d:
+        cells = int(np.prod(shape))
+        work = args.steps * cells * sample
+        how = (f"each bench step = {sample} time step of the whole {shape[2]}x{shape[1]}x{shape[0]} grid, split "
+               f"into {n_proc} z-slabs stepped concurrently by the reference's FDTD.step() in {n_proc} processes "
+               f"(its NumPy backend, 3-D update and source loop; no plane monitors); float64/complex128")
+    else:
+        shape = res[0][2]
+        cells = int(np.prod(shape))
+        work = n_proc * args.steps * cells * sample
+        how = (f"each bench step = {sample} time steps of the whole workload (reference FDTD.step(): NumPy "
+               f"backend, source loop, line monitors) in each of {n_proc} processes, one per host core; "
+               f"float64/complex128")
+    value = work / el / 1e9
+    n_steps = len(t)
     line = {"impl": "reference", "metric": METRIC, "value": round(value, 5), "unit": UNIT, "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(el / args.steps * 1e3, 3),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": desc, "grid": shape, "time_steps_per_step": sample,
-                       "parallelism": f"{n_proc} concurrent copies of the NumPy loop, one per host core"},
-            "cpu_baseline": {"value": round(value, 5), "unit": UNIT, "cores": n_proc, "kind": "port",
-                             "sample": f"{sample} time steps of the workload per bench step in each of {n_proc} "
-                                       f"processes, float64 NumPy; value = all processes' cell updates over the "
-                                       f"slowest one's time"},
+            "config": _config(args.workload, shape, n_steps, args.gpus),
+            "cpu_baseline": {"value": round(value, 5), "unit": UNIT, "cores": n_proc, "kind": "reference",
+                             "sample": how + "; value = cell updates over the slowest process's time"},
             "e2e": {"value": round(value, 5), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
 
-def _reference_worker(name, n_steps, steps, warmup, barrier, q):
-    """One copy of the reference arm's sample: its own workload and host grid, `warmup`
-    untimed samples, then `steps` timed ones started together with the other copies."""
+def _reference_worker(name, n_steps, job, sample, steps, warmup, barrier, q):
+    """One process of the reference arm: builds the workload with the reference package,
+    runs `warmup` untimed bench steps, then `steps` timed ones started together with the
+    other processes; puts (seconds, cells, grid shape) on the queue."""
     try:
-        from oracle import fdtd2d
+        _quiet_child()
+        api = reference_api()
+        Wm = workload_module()
+        kw = {} if n_steps is None else {"n_steps": n_steps}
+        kind, zr, tmp = job
+        if kind == "3d":
+            d, t, dx = getattr(Wm, name)(api=api, monitors=False, **kw)
+            sim = _reference_slab_sim(api, d, t, dx, zr, tmp)
+        else:
+            d, t, dx = getattr(Wm, name)(api=api, **kw)
+            grid = api.RegularGrid(d, dx)
+            sim = api.FDTD(design=grid, time=t)
+        sim.initialize_simulation(save=False, live=False, save_memory_mode=True)
+        shape = list(np.shape(sim.mesh.permittivity))
 
-        d, t, dx, _ = workload(name, n_steps)
-        eps, sig = _host_grid(d, dx)
-        sample = max(1, min(20, len(t)))
+        def bench_step():
+            for _ in range(sample):
+                if sim.current_step >= sim.num_steps:
+                    sim.initialize_simulation(save=False, live=False, save_memory_mode=True)
+                sim.step()
+
         for _ in range(warmup):
-            fdtd2d.run(eps, sig, dx, dx, t[1] - t[0], sample, d.sources, d.monitors, record=True)
+            bench_step()
         barrier.wait()
         t0 = time.perf_counter()
         for _ in range(steps):
-            fdtd2d.run(eps, sig, dx, dx, t[1] - t[0], sample, d.sources, d.monitors, record=True)
-        q.put((time.perf_counter() - t0, eps.size, sample, list(eps.shape)))
-    except Exception:  # noqa: BLE001 - reported by the parent as unavailable
+            bench_step()
+        q.put((time.perf_counter() - t0, int(np.prod(shape)), shape))
+    except Exception as e:  # noqa: BLE001 - reported by the parent as unavailable
         try:
             barrier.abort()
         finally:
-            q.put(None)
+            q.put(f"{type(e).__name__}: {e}")
 
 
-def _host_grid(d, dx):
-    """Material arrays for the CPU arm from the oracle's host rasteriser (the
-    reference's meshing restated; bit-identical to the GPU rasteriser's output)."""
-    from oracle import raster2d
-
-    return raster2d.rasterize(d, dx)
+def _reference_slab_sim(api, d, t, dx, zr, tmp):
+    """The reference FDTD on planes [z0, z1) of the 3D grid: a RegularGrid3D holding that
+    slab's material (the grid from the extruding restatement of the reference's
+    rasteriser, oracle/raster3d.py) and the design's source with only the profile points
+    whose plane lies in the slab, shifted to slab coordinates."""
+    z0, z1 = zr
+    eps = np.array(np.load(os.path.join(tmp, "eps.npy"), mmap_mode="r")[z0:z1])
+    sig = np.array(np.load(os.path.join(tmp, "sig.npy"), mmap_mode="r")[z0:z1])
+    mesh = api.RegularGrid3D.__new__(api.RegularGrid3D)
+    mesh.design = d
+    mesh.resolution = mesh.resolution_xy = mesh.resolution_z = dx
+    mesh.dx = mesh.dy = mesh.dz = dx
+    mesh.permittivity, mesh.permeability, mesh.conductivity = eps, np.ones_like(eps), sig
+    mesh.shape = eps.shape
+    for src in d.sources:
+        if hasattr(src, "mode_profiles"):
+            pts = []
+            for p in src.mode_profiles[0]:
+                k = int(round(p[3] / dx))
+                if z0 <= k < z1:
+                    pts.append([p[0], p[1], p[2], p[3] - z0 * dx])
+            src.mode_profiles[0] = pts
+    return api.FDTD(design=mesh, time=t)
 
 
 def run_topo(args):

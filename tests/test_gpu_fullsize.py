@@ -1,13 +1,14 @@
-"""The benchmark configurations at their full sizes: float32 against a float64 run of
-the same workload on the GPU (the float64 path matches the reference's own runs to
-1e-11 on the golden fixtures), through the quantities each configuration reports.
+"""The benchmark configurations at their full sizes and lengths: float32 against a float64
+run of the same workload on the GPU (the float64 path matches the CPU oracle to 1e-11 on
+these grids, tests/test_gpu_parity_configs.py), through the fields after the last step
+and the quantities each configuration reports.
 
-* 2D dipole, 400 x 400, 2000 steps: monitor time series within 1e-5 of their peak;
-  integrated edge power within 1e-4.
-* 2D MMI, 2000 x 1000, 20000 steps (CW): per-port, per-wavelength transmission
-  |dT| <= 1e-4; final field relative L2 <= 1e-4.
-* 3D SOI MMI, 600 x 300 x 150, 8000 steps: port flux at every wavelength within 1e-4
-  of the largest port flux.
+* 2D MMI, 2000 x 1000, 20000 steps (CW): relative L2 of (Ez, Hx, Hy) <= 1e-5;
+  per-port, per-wavelength transmission |dT| <= 1e-4.
+* 3D SOI MMI, 600 x 300 x 150, 8000 steps: relative L2 of the six components <= 1e-5;
+  port flux at every wavelength within 1e-4 of the largest port flux.
+
+The measured errors are printed (``pytest -s``) and carried in the assertion messages.
 """
 import numpy as np
 import pytest
@@ -29,35 +30,36 @@ def _mon(sim, name):
     return next(m for m in sim.monitors if m.name == name)
 
 
-def test_dipole_full_size_fp32_matches_fp64(bz):
-    s32, s64 = _run(bz, "dipole_2d", "fp32"), _run(bz, "dipole_2d", "fp64")
-    for name in ("left", "right", "bottom", "top"):
-        a, b = _mon(s32, name), _mon(s64, name)
-        ez32, ez64 = np.array(a.fields["Ez"]), np.array(b.fields["Ez"])
-        assert ez32.shape == ez64.shape and ez32.shape[0] == 2000
-        assert np.abs(ez32 - ez64).max() <= 1e-5 * np.abs(ez64).max(), name
-        p32, p64 = np.sum(a.power_history), np.sum(b.power_history)
-        assert abs(p32 - p64) <= 1e-4 * abs(p64), name
+def _rel(s32, s64, keys):
+    num = den = 0.0
+    for k in keys:
+        a = s32.engine.field(k).double()
+        b = s64.engine.field(k)
+        num += float((a - b).square().sum())
+        den += float(b.square().sum())
+    return (num / den) ** 0.5
 
 
-def test_mmi_full_size_fp32_transmission_matches_fp64(bz):
+def test_mmi_full_size_fp32_matches_fp64(bz):
     s32, s64 = _run(bz, "mmi_2d", "fp32"), _run(bz, "mmi_2d", "fp64")
     T = {}
     for prec, sim in (("fp32", s32), ("fp64", s64)):
         fin = _mon(sim, "in").flux()
         T[prec] = np.array([_mon(sim, p).flux() / fin for p in ("port_top", "port_bottom")])
     dT = np.abs(T["fp32"] - T["fp64"]).max()
-    print(f"MMI max |dT| fp32 vs fp64 = {dT:.2e}; T = {np.round(T['fp64'], 4)}")
-    assert dT <= 1e-4
-    e32 = s32.engine.field("Ez").cpu().numpy().astype(np.float64)
-    e64 = s64.engine.field("Ez").cpu().numpy()
-    assert np.linalg.norm(e32 - e64) <= 1e-4 * np.linalg.norm(e64)
+    err = _rel(s32, s64, ("Ez", "Hx", "Hy"))
+    print(f"MMI 20000 steps: fields relative L2 fp32 vs fp64 {err:.2e}; max |dT| {dT:.2e}; "
+          f"T = {np.round(T['fp64'], 4)}")
+    assert dT <= 1e-4, f"MMI max |dT| {dT:.3e}"
+    assert err <= 1e-5, f"MMI fields relative L2 {err:.3e}"
 
 
-def test_soi_3d_full_size_fp32_flux_matches_fp64(bz):
+def test_soi_3d_full_size_fp32_matches_fp64(bz):
     s32, s64 = _run(bz, "soi_mmi_3d", "fp32"), _run(bz, "soi_mmi_3d", "fp64")
     f32 = np.array([_mon(s32, p).flux() for p in ("port_top", "port_bottom")])
     f64 = np.array([_mon(s64, p).flux() for p in ("port_top", "port_bottom")])
-    err = np.abs(f32 - f64).max() / np.abs(f64).max()
-    print(f"3D port flux max relative difference fp32 vs fp64 = {err:.2e}")
-    assert np.abs(f64).max() > 0 and err <= 1e-4
+    ferr = np.abs(f32 - f64).max() / np.abs(f64).max()
+    err = _rel(s32, s64, ("Ex", "Ey", "Ez", "Hx", "Hy", "Hz"))
+    print(f"3D SOI MMI 8000 steps: fields relative L2 fp32 vs fp64 {err:.2e}; port flux {ferr:.2e}")
+    assert np.abs(f64).max() > 0 and ferr <= 1e-4, f"3D port flux relative difference {ferr:.3e}"
+    assert err <= 1e-5, f"3D fields relative L2 {err:.3e}"

@@ -36,6 +36,28 @@ def test_rasterizer3d_extrude_mode_fills_thickness(bz):
     assert grid.conductivity[0].max() > 0 and grid.conductivity[-1].max() > 0  # z-face PML
 
 
+@pytest.mark.parametrize("which", ["stack", "soi_mmi_3d"])
+def test_rasterizer3d_extrude_mode_bit_exact_vs_oracle(bz, which):
+    """extrude=True against the oracle's restatement (the reference's 27-sample rule
+    with the structure's z range tested, plus z-face PML), bit for bit: the small
+    stack of the fixtures and the full 600 x 300 x 150 SOI MMI grid of the 3D
+    workload."""
+    from oracle import raster3d
+    from beamz_b200 import workloads as W
+
+    if which == "stack":
+        d, res = D.design_3d(bz), D.RES
+    else:
+        d, _, res = W.soi_mmi_3d()
+    grid = bz.RegularGrid3D(d, res, extrude=True)
+    eps, mu, sig = raster3d.rasterize3d(d, res, extrude=True)
+    assert grid.permittivity.shape == eps.shape
+    np.testing.assert_array_equal(grid.permittivity, eps)
+    np.testing.assert_array_equal(grid.permeability, mu)
+    np.testing.assert_array_equal(grid.conductivity, sig)
+    assert sig[0].max() > 0 and sig[-1].max() > 0
+
+
 def _golden_3d(bz, golden, precision):
     g = golden("step3d")
     d = D.step3d_design(bz)

@@ -56,6 +56,32 @@ def test_oracle_rasteriser_matches_reference(bz, golden, name):
     np.testing.assert_array_equal(sig, g["sigma"])
 
 
+def test_oracle_rasteriser3d_matches_reference(bz, golden):
+    """The 3D restatement in its reference mode reproduces RegularGrid3D's grids
+    (z-collapsed bounding boxes, 2D PML over every layer) bit for bit."""
+    import designs as D
+    from oracle import raster3d
+
+    g = golden("raster3d")
+    eps, mu, sig = raster3d.rasterize3d(D.design_3d(bz), D.RES)
+    np.testing.assert_array_equal(eps, g["eps"])
+    np.testing.assert_array_equal(mu, g["mu"])
+    np.testing.assert_array_equal(sig, g["sigma"])
+
+
+def test_oracle_rasteriser3d_extrude_fills_layers(bz):
+    """extrude=True fills each structure's [z, z + depth) and grades the z faces."""
+    import designs as D
+    from oracle import raster3d
+
+    eps, mu, sig = raster3d.rasterize3d(D.design_3d(bz), D.RES, extrude=True)
+    i, j = int(0.6e-6 / D.RES), int(0.3e-6 / D.RES)
+    assert np.all(eps[:8, i, j] == 2.085) and np.all(eps[8:12, i, j] == 12.25) and np.all(eps[13:, i, j] == 1.0)
+    ref_eps, _, ref_sig = raster3d.rasterize3d(D.design_3d(bz), D.RES)
+    assert not np.array_equal(eps, ref_eps)
+    assert sig[0].max() > 0 and sig[-1].max() > 0 and sig[len(sig) // 2].max() <= ref_sig.max() + 1e-9
+
+
 def _step3d_setup(bz, golden):
     import designs as D
 
