@@ -1,177 +1,147 @@
-"""Topology-optimisation building blocks (beamz/optimization/topology.py:22-306).
+"""Density filters and the masked density update of a topology loop, on torch tensors
+batched over designs (the operations of beamz/optimization/topology.py:31-178).
 
-Density arrays live on the host as NumPy float64 (they are small: one value per
-design-region cell). The masked box blur, sigmoid projection, masked update with
-clipping, Adam step and overlap gradient follow the reference's definitions.
+Every function takes densities shaped ``(..., H, W)`` -- one design or a batch of
+designs sharing leading dimensions -- as NumPy arrays or torch tensors. The arithmetic
+runs in float64 on the tensor's device (a CUDA batch stays on the GPU), and the result
+comes back as the kind of array that was passed in.
+
+* ``masked_box_blur``: normalised box average over a (2r+1)^2 window counting only
+  cells inside the mask; values are continued past the border by their edge value,
+  the mask by zeros; a window holding no mask cell divides by one.
+* ``apply_density_update``: ``clip(rho + lr * g_s, 0, 1)`` inside the mask, where
+  ``g_s`` is the gradient restricted to the mask and optionally smoothed; returns the
+  new density, ``g_s``, the change, and the L2 norm and largest magnitude of the
+  change inside the mask (floats for one design, one value per design for a batch).
+* ``blur_density``: separable box filter with zero padding ('same' size).
+* ``project_density``: logistic projection ``1 / (1 + exp(-beta (rho - eta)))``.
+* ``compute_overlap_gradient``: ``Re(conj(E_adj) E_fwd)`` over the common extent.
+
+The exact discrete adjoint gradient of a monitor objective is
+``beamz_b200.optimization.adjoint``; the tanh-projected filter chain of the topology
+loop is ``beamz_b200.optimization.topo2d``.
 """
 from __future__ import annotations
 
-from typing import Callable, Optional, Tuple
+from typing import Callable, Optional
 
 import numpy as np
-from numpy.lib.stride_tricks import sliding_window_view
-
-from .optimizers import Optimizer
-
-DensityArray = np.ndarray
-MaskArray = np.ndarray
+import torch
+import torch.nn.functional as F
 
 
-def _validate_shapes(density, gradient, mask) -> None:
-    if density.shape != gradient.shape:
-        raise ValueError("Gradient and density must share shape.")
-    if mask.shape != density.shape:
-        raise ValueError("Mask must share the same shape as density.")
+def _tensor(x, device=None) -> torch.Tensor:
+    if isinstance(x, torch.Tensor):
+        return x.to(dtype=torch.float64, device=device if device is not None else x.device)
+    return torch.as_tensor(np.asarray(x, dtype=np.float64), device=device)
 
 
-def _masked_box_blur(values, mask, radius):
-    """Mean over the (2r+1)^2 window of the cells inside ``mask`` (edge-padded values,
-    zero-padded mask); windows with no mask cell return the weighted sum over 1."""
-    radius = int(max(0, round(radius)))
-    if radius < 1:
+def _like(t: torch.Tensor, template):
+    return t if isinstance(template, torch.Tensor) else t.cpu().numpy()
+
+
+def _planes(t: torch.Tensor) -> tuple[torch.Tensor, tuple]:
+    """(N, 1, H, W) view of a (..., H, W) tensor, and the leading shape."""
+    lead = tuple(t.shape[:-2])
+    return t.reshape((-1, 1) + tuple(t.shape[-2:])), lead
+
+
+def _box_sum(x: torch.Tensor, r: int) -> torch.Tensor:
+    """Sum over the (2r+1)^2 window of an already padded (N, 1, H+2r, W+2r) tensor."""
+    k = torch.ones((1, 1, 2 * r + 1, 2 * r + 1), dtype=x.dtype, device=x.device)
+    return F.conv2d(x, k)
+
+
+def masked_box_blur(values, mask, radius):
+    """Normalised box average of ``values`` over the cells of ``mask`` (see module)."""
+    r = int(max(0, round(radius)))
+    if r < 1:
         return values
-    pv = np.pad(values, radius, mode="edge")
-    pm = np.pad(mask.astype(float), radius, mode="constant", constant_values=0.0)
-    win = (2 * radius + 1, 2 * radius + 1)
-    vv, mv = sliding_window_view(pv, win), sliding_window_view(pm, win)
-    num = (vv * mv).sum(axis=(-2, -1))
-    den = mv.sum(axis=(-2, -1))
-    return num / np.where(den == 0.0, 1.0, den)
+    v = _tensor(values)
+    m = _tensor(mask, device=v.device).expand_as(v)
+    vp, lead = _planes(v)
+    mp, _ = _planes(m)
+    num = _box_sum(F.pad(vp, (r, r, r, r), mode="replicate") * F.pad(mp, (r, r, r, r)), r)
+    den = _box_sum(F.pad(mp, (r, r, r, r)), r)
+    out = (num / torch.where(den == 0, torch.ones_like(den), den)).reshape(v.shape)
+    return _like(out, values)
 
 
 def apply_density_update(density, gradient, mask, *, learning_rate: float, blur_radius: int = 0,
-                         blur_fn: Optional[Callable] = None) -> Tuple[np.ndarray, np.ndarray, np.ndarray, float, float]:
-    """``clip(density + lr * smooth(gradient inside mask), 0, 1)`` inside ``mask``.
-
-    Returns (new_density, applied_gradient, density_delta, change_norm, max_update).
-    """
-    _validate_shapes(density, gradient, mask)
-    g = np.where(mask, gradient, 0.0).astype(float, copy=False)
+                         blur_fn: Optional[Callable] = None):
+    """Masked, clipped density step (see module). Returns
+    ``(new_density, applied_gradient, delta, change_norm, max_update)``."""
+    rho = _tensor(density)
+    g = _tensor(gradient, device=rho.device)
+    if g.shape != rho.shape:
+        raise ValueError(f"gradient shape {tuple(g.shape)} differs from density shape {tuple(rho.shape)}")
+    m = torch.as_tensor(np.asarray(mask) if not isinstance(mask, torch.Tensor) else mask, device=rho.device)
+    if m.shape != rho.shape[-m.dim():] or m.dim() < 2:
+        raise ValueError(f"mask shape {tuple(m.shape)} does not match density shape {tuple(rho.shape)}")
+    m = m.to(torch.bool).expand_as(rho)
+    zero = torch.zeros((), dtype=rho.dtype, device=rho.device)
+    gs = torch.where(m, g, zero)
     if blur_fn is not None:
-        sm = blur_fn(g, mask)
+        gs = _tensor(blur_fn(_like(gs, density), _like(m, density)), device=rho.device)
     elif blur_radius > 0:
-        sm = _masked_box_blur(g, mask, blur_radius)
+        gs = _tensor(masked_box_blur(gs, m.to(rho.dtype), blur_radius))
+    gs = torch.where(m, gs, zero)
+    new = torch.where(m, torch.clamp(rho + learning_rate * gs, 0.0, 1.0), rho)
+    delta = torch.where(m, new - rho, zero)
+    flat = delta.reshape(delta.shape[:-2] + (-1,))
+    norm = torch.linalg.vector_norm(flat, dim=-1)
+    peak = flat.abs().amax(dim=-1) if flat.shape[-1] else torch.zeros(flat.shape[:-1], dtype=rho.dtype)
+    if rho.dim() == 2:
+        norm, peak = float(norm), float(peak)
     else:
-        sm = g
-    sm = np.where(mask, sm, 0.0)
-    new = np.where(mask, np.clip(density + learning_rate * sm, 0.0, 1.0), density)
-    delta = np.where(mask, new - density, 0.0)
-    if np.any(mask):
-        change_norm = float(np.linalg.norm(delta[mask]))
-        max_update = float(np.max(np.abs(delta[mask])))
-    else:
-        change_norm = max_update = 0.0
-    return new, sm, delta, change_norm, max_update
+        norm, peak = _like(norm, density), _like(peak, density)
+    return _like(new, density), _like(gs, density), _like(delta, density), norm, peak
 
 
-def initialize_density_from_region(design_region, resolution: float) -> DensityArray:
-    width = getattr(design_region, "width", None)
-    height = getattr(design_region, "height", None)
-    if width is None or height is None:
-        raise ValueError("Design region must expose width and height attributes.")
-    nx = max(1, int(round(width / resolution)))
-    ny = max(1, int(round(height / resolution)))
-    density = np.full((ny, nx), 0.5, dtype=float)
-    grid = getattr(getattr(design_region, "material", None), "permittivity_grid", None)
-    if grid is not None:
-        density = _resample_to_shape(grid, (ny, nx))
-    return density
-
-
-def blur_density(density, radius: float, *, backend: str = "numpy") -> DensityArray:
-    """Separable box blur (``np.convolve`` 'same' along rows then columns)."""
+def blur_density(density, radius: float, *, backend: str = "torch"):
+    """Separable (2r+1)-point box filter along x then y, zero padded, same size."""
     r = max(0, int(round(radius)))
     if r <= 0:
         return density
-    k = np.ones((2 * r + 1,), dtype=float)
-    k /= k.size
-    out = np.apply_along_axis(lambda row: np.convolve(row, k, mode="same"), axis=1, arr=density)
-    return np.apply_along_axis(lambda col: np.convolve(col, k, mode="same"), axis=0, arr=out)
+    t = _tensor(density)
+    p, _ = _planes(t)
+    k = torch.full((1, 1, 1, 2 * r + 1), 1.0 / (2 * r + 1), dtype=t.dtype, device=t.device)
+    p = F.conv2d(F.pad(p, (r, r, 0, 0)), k)
+    p = F.conv2d(F.pad(p, (0, 0, r, r)), k.transpose(-1, -2))
+    return _like(p.reshape(t.shape), density)
 
 
-def project_density(density, beta: float, eta: float) -> DensityArray:
+def project_density(density, beta: float, eta: float):
+    """Logistic projection towards 0/1 around eta; beta <= 0 leaves the density as is."""
     if beta <= 0:
         return density
-    return 1.0 / (1.0 + np.exp(-beta * (density - eta)))
+    t = _tensor(density)
+    return _like(torch.sigmoid(beta * (t - eta)), density)
 
 
-def compute_overlap_gradient(forward_fields, adjoint_fields, *, monitor=None) -> DensityArray:
-    """Re(conj(adjoint Ez) * forward Ez) over the common extent of the two fields."""
-    fwd = _extract_field(forward_fields, "Ez")
-    adj = _extract_field(adjoint_fields, "Ez")
-    if fwd is None or adj is None:
-        raise ValueError("Forward/adjoint data must contain an 'Ez' entry.")
-    fwd, adj = np.asarray(fwd), np.asarray(adj)
-    g = np.real(np.conj(adj) * fwd)
-    return g[tuple(slice(0, min(a, b)) for a, b in zip(fwd.shape, adj.shape))]
-
-
-def run_forward(sim, source, monitor, *, live: bool = False):
-    sim.sources = [source]
-    sim.initialize_simulation(save=True, live=live)
-    while sim.step():
-        pass
-    return sim.finalize_simulation()
-
-
-def run_adjoint(density, sim, source, forward_results, monitor=None, *, live: bool = False) -> DensityArray:
-    """Runs the adjoint simulation and returns a zero gradient, as the reference's
-    placeholder does (topology.py:191-207). The exact discrete adjoint of this
-    package is ``beamz_b200.optimization.adjoint``."""
-    sim.sources = [source]
-    sim.initialize_simulation(save=True, live=live)
-    while sim.step():
-        pass
-    sim.finalize_simulation()
-    return np.zeros_like(density, dtype=float)
-
-
-def compute_objective(results, monitor=None) -> float:
-    ez = _extract_field(results, "Ez")
-    return 0.0 if ez is None else float(np.sum(np.abs(ez) ** 2))
-
-
-def apply_optimizer_step(density, gradient, optimizer_state, *, method="adam", learning_rate=1e-2, **kwargs):
-    if gradient.shape != density.shape:
-        raise ValueError("Gradient and density must share shape.")
-    opt = Optimizer(method=method, learning_rate=learning_rate, options=kwargs) if optimizer_state is None \
-        else optimizer_state["optimizer"]
-    return np.clip(density + opt.step(gradient), 0.0, 1.0), {"optimizer": opt}
-
-
-def update_design_region_material(design_region, density) -> None:
-    material = getattr(design_region, "material", None)
-    if material is None or not hasattr(material, "update_grid"):
-        return
-    material.update_grid("permittivity", np.interp(density, [0.0, 1.0], [_background_eps(), _target_eps()]))
-
-
-def _normalize_to_unit_interval(values):
-    lo, hi = values.min(), values.max()
-    return np.zeros_like(values) if np.isclose(lo, hi) else (values - lo) / (hi - lo)
-
-
-def _resample_to_shape(grid, shape):
-    ny, nx = shape
-    ys, yd = np.linspace(0.0, 1.0, grid.shape[0]), np.linspace(0.0, 1.0, ny)
-    xs, xd = np.linspace(0.0, 1.0, grid.shape[1]), np.linspace(0.0, 1.0, nx)
-    tmp = np.stack([np.interp(yd, ys, grid[:, c]) for c in range(grid.shape[1])], axis=1)
-    out = np.stack([np.interp(xd, xs, tmp[r, :]) for r in range(ny)], axis=0)
-    return _normalize_to_unit_interval(out)
-
-
-def _background_eps() -> float:
-    return 1.444 ** 2
-
-
-def _target_eps() -> float:
-    return 2.25 ** 2
-
-
-def _extract_field(container, key):
+def _ez(container):
     if container is None:
         return None
-    if isinstance(container, dict):
-        v = container.get(key)
-        return v[-1] if isinstance(v, list) and v else v
-    return getattr(container, key, None)
+    v = container.get("Ez") if isinstance(container, dict) else getattr(container, "Ez", None)
+    if isinstance(v, (list, tuple)):
+        v = v[-1] if v else None
+    return v
+
+
+def compute_overlap_gradient(forward_fields, adjoint_fields, *, monitor=None):
+    """Re(conj(E_adj) * E_fwd) of the two runs' Ez (a dict or object with ``Ez``; a list
+    holds snapshots, the last is used), over the extent common to both."""
+    fwd, adj = _ez(forward_fields), _ez(adjoint_fields)
+    if fwd is None or adj is None:
+        raise ValueError("forward and adjoint results both need an 'Ez' field")
+    ft = torch.as_tensor(fwd) if isinstance(fwd, torch.Tensor) else torch.as_tensor(np.asarray(fwd))
+    at = torch.as_tensor(adj, device=ft.device) if isinstance(adj, torch.Tensor) else \
+        torch.as_tensor(np.asarray(adj), device=ft.device)
+    common = tuple(slice(0, min(a, b)) for a, b in zip(ft.shape, at.shape))
+    ft, at = ft[common], at[common]
+    g = (at.conj() * ft).real if (ft.is_complex() or at.is_complex()) else at * ft
+    return _like(g.to(torch.float64), fwd)
+
+
+__all__ = ["masked_box_blur", "apply_density_update", "blur_density", "project_density",
+           "compute_overlap_gradient"]

@@ -142,19 +142,89 @@ def test_apply_density_update_zero_gradient_returns_no_change():
     assert norm == 0.0 and mx == 0.0
 
 
-def test_masked_blur_and_adam():
-    from beamz_b200.optimization.optimizers import Optimizer
-    from beamz_b200.optimization.topology import _masked_box_blur
+def test_masked_blur_matches_window_loop():
+    """masked_box_blur against an explicit window loop (edge-continued values, zero
+    mask outside, empty windows divided by one), on a ragged mask."""
+    from beamz_b200.optimization.topology import masked_box_blur
 
-    v = np.arange(25.0).reshape(5, 5)
-    m = np.ones((5, 5), bool)
-    b = _masked_box_blur(v, m, 1)
-    assert b[2, 2] == pytest.approx(12.0)
-    opt = Optimizer(learning_rate=0.1)
-    u = opt.step(np.array([1.0, -2.0]))
-    np.testing.assert_allclose(u, [-0.1, 0.1], rtol=1e-6)
+    rng = np.random.default_rng(3)
+    v = rng.random((6, 7))
+    m = rng.random((6, 7)) > 0.4
+    m[0, :] = False
+    r = 1
+    vp = np.pad(v, r, mode="edge")
+    mp = np.pad(m.astype(float), r)
+    want = np.zeros_like(v)
+    for i in range(6):
+        for j in range(7):
+            w = mp[i:i + 3, j:j + 3]
+            den = w.sum()
+            want[i, j] = (vp[i:i + 3, j:j + 3] * w).sum() / (den if den else 1.0)
+    np.testing.assert_allclose(masked_box_blur(v, m, r), want, rtol=1e-14)
+    assert masked_box_blur(np.arange(25.0).reshape(5, 5), np.ones((5, 5), bool), 1)[2, 2] == pytest.approx(12.0)
+
+
+def test_density_update_batched_equals_per_design():
+    """A batch of designs (leading dimension) gives each design's own update."""
+    import torch
+
+    from beamz_b200.optimization.topology import apply_density_update
+
+    rng = np.random.default_rng(5)
+    rho, g = rng.random((4, 9, 8)), rng.standard_normal((4, 9, 8))
+    mask = rng.random((9, 8)) > 0.3
+    new_b, app_b, d_b, n_b, mx_b = apply_density_update(torch.as_tensor(rho), torch.as_tensor(g), mask,
+                                                        learning_rate=0.3, blur_radius=1)
+    assert isinstance(new_b, torch.Tensor) and n_b.shape == (4,)
+    for b in range(4):
+        new, app, dl, n, mx = apply_density_update(rho[b], g[b], mask, learning_rate=0.3, blur_radius=1)
+        np.testing.assert_allclose(new_b[b].numpy(), new, rtol=1e-14)
+        np.testing.assert_allclose(app_b[b].numpy(), app, rtol=1e-14)
+        assert float(n_b[b]) == pytest.approx(n) and float(mx_b[b]) == pytest.approx(mx)
+        assert np.all(new[~mask] == rho[b][~mask]) and np.all((new >= 0) & (new <= 1))
+
+
+def test_adam_steps_follow_the_published_rule():
+    """Three Adam steps against the bias-corrected moment formulas written out here."""
+    import torch
+
+    from beamz_b200.optimization.optimizers import Optimizer
+
+    rng = np.random.default_rng(7)
+    grads = [rng.standard_normal((2, 3)) for _ in range(3)]
+    opt = Optimizer(learning_rate=0.05, options={"beta1": 0.8, "beta2": 0.99})
+    m = v = np.zeros((2, 3))
+    for t, g in enumerate(grads, start=1):
+        m = 0.8 * m + 0.2 * g
+        v = 0.99 * v + 0.01 * g * g
+        want = -0.05 * (m / (1 - 0.8 ** t)) / (np.sqrt(v / (1 - 0.99 ** t)) + 1e-8)
+        np.testing.assert_allclose(opt.step(g), want, rtol=1e-12)
+    np.testing.assert_allclose(Optimizer(learning_rate=0.1).step(np.array([1.0, -2.0])), [-0.1, 0.1], rtol=1e-6)
+    out = Optimizer().step(torch.ones(3))
+    assert isinstance(out, torch.Tensor)
+    assert Optimizer().step(np.zeros(0)).shape == (0,)
     with pytest.raises(ValueError):
-        Optimizer(method="sgd")
+        Optimizer(method="lbfgs")
+    with pytest.raises(TypeError):
+        Optimizer().step([1.0, 2.0])
+
+
+def test_filters_and_overlap_gradient():
+    from beamz_b200.optimization.topology import blur_density, compute_overlap_gradient, project_density
+
+    rho = np.zeros((5, 5))
+    rho[2, 2] = 9.0
+    b = blur_density(rho, 1)
+    np.testing.assert_allclose(b[1:4, 1:4], np.ones((3, 3)))
+    assert b.sum() == pytest.approx(9.0)
+    p = project_density(np.array([0.5, 1.0]), 10.0, 0.5)
+    assert p[0] == pytest.approx(0.5) and p[1] == pytest.approx(1 / (1 + np.exp(-5.0)))
+    fwd = {"Ez": [np.ones((3, 4)) * (1 + 1j)]}
+    adj = {"Ez": np.full((2, 5), 2.0 + 0j)}
+    g = compute_overlap_gradient(fwd, adj)
+    assert g.shape == (2, 4) and np.allclose(g, 2.0)
+    with pytest.raises(ValueError):
+        compute_overlap_gradient({}, adj)
 
 
 @pytest.mark.parametrize("save,memory,cache,decimate,n", [(False, True, [], 1, 20000), (True, False, [], 1, 20000),
