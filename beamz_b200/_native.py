@@ -73,8 +73,8 @@ class Gemm(C.Structure):
 
 class Grid3D(C.Structure):
     _fields_ = [("nx", i32), ("ny", i32), ("nz", i32), ("pitch", i32), ("n_designs", i32), ("n_comp", i32),
-                ("n_mat", i32), ("dtype", i32), ("tile_z", i32), ("tile_y", i32), ("chx", f64), ("chy", f64),
-                ("chz", f64), ("qx", f64), ("qz", f64), ("inv_kd2", f64)]
+                ("n_mat", i32), ("dtype", i32), ("tile_z", i32), ("tile_y", i32), ("x_cells", i32),
+                ("chx", f64), ("chy", f64), ("chz", f64), ("qx", f64), ("qz", f64), ("inv_kd2", f64)]
 
 
 class Fields3D(C.Structure):
@@ -148,12 +148,15 @@ _adam = _sig("bz_adam", C.c_int, [vp, vp, vp, vp, vp, i64, C.c_float, C.c_float,
                                   C.c_float, vp])
 _to_bf16 = _sig("bz_to_bf16", C.c_int, [vp, vp, i64, vp])
 _gemm_err = _sig("bz_gemm_error", C.c_int, [C.POINTER(i32), i32])
+_gemm_selftest = _sig("bz_gemm_wait_selftest", C.c_int, [vp, vp, vp, i32, vp])
+_field_check = _sig("bz_field_check", C.c_int, [vp, i32, i64, f64, i64, vp, vp])
 
 #: every symbol include/beamz_b200.h declares (checked by the CPU test suite)
 EXPORTED = ["bz_version", "bz_last_error", "bz_step2d", "bz_step2d_multi", "bz_dft_fold", "bz_step2d_dft_static", "bz_advance_step",
             "bz_adjoint_step2d", "bz_adjoint_step2d_multi", "bz_step3d", "bz_cell_ops", "bz_gather", "bz_power3d", "bz_dft_fold_q", "bz_rasterize3d", "bz_prepare_coeffs", "bz_update_h2d",
             "bz_update_e2d", "bz_rasterize2d", "bz_gemm_bf16", "bz_spectral_mix", "bz_spectral_mix_bwd", "bz_gelu_bwd",
-            "bz_row_mean", "bz_row_broadcast", "bz_chan_sum", "bz_adam", "bz_to_bf16", "bz_gemm_error"]
+            "bz_row_mean", "bz_row_broadcast", "bz_chan_sum", "bz_adam", "bz_to_bf16", "bz_gemm_error",
+            "bz_gemm_wait_selftest", "bz_field_check"]
 
 
 class NativeError(RuntimeError):
@@ -280,6 +283,15 @@ def adam(w, g, m, v, wh, n, lr, b1, b2, eps, step, wd, stream) -> None:
 
 def to_bf16(x, y, n, stream) -> None:
     check(_to_bf16(x, y, n, stream))
+
+
+def field_check(ptr: int, dtype: int, n: int, limit: float, step: int, status_ptr: int, stream) -> None:
+    check(_field_check(vp(ptr), dtype, n, float(limit), int(step), vp(status_ptr), vp(stream)))
+
+
+def gemm_wait_selftest(a_ptr: int, b_ptr: int, c_ptr: int, wait_limit: int, stream) -> int:
+    """Status of the tcgen05 GEMM's withheld-slice run (BZ_ERR_TIMEOUT expected); does not raise."""
+    return _gemm_selftest(vp(a_ptr), vp(b_ptr), vp(c_ptr), int(wait_limit), vp(stream))
 
 
 def gemm_error(reset: bool = True) -> int:

@@ -50,3 +50,41 @@ extern "C" int bz_advance_step(int64_t* d_step, int64_t n, void* stream) {
   advance_step_kernel<<<1, 1, 0, bz::as_stream(stream)>>>(d_step, n);
   return bz::check_launch("bz_advance_step");
 }
+
+// ---- divergence check ------------------------------------------------------------
+// One pass over a field array: a value that is not finite or whose magnitude exceeds
+// `limit` marks the run as diverged. The first detection of a launch writes
+// BZ_ERR_DIVERGED into status[0] and the step into status[1]; later launches leave a
+// recorded detection in place. The host reads the words when it next synchronizes.
+namespace {
+template <typename T>
+__global__ void field_check_kernel(const T* __restrict__ f, long long n, double limit, long long step,
+                                   long long* __restrict__ status) {
+  bool bad = false;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const double v = (double)__ldg(f + i);
+    bad |= !(fabs(v) <= limit);  // NaN compares false
+  }
+  if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) {
+    if (atomicCAS(reinterpret_cast<unsigned long long*>(status), 0ull, (unsigned long long)(long long)BZ_ERR_DIVERGED) == 0ull)
+      status[1] = step;
+  }
+}
+}  // namespace
+
+extern "C" int bz_field_check(const void* field, int32_t dtype, int64_t n, double limit, int64_t step,
+                              int64_t* status, void* stream) {
+  BZ_REQUIRE(field && status, "bz_field_check: NULL field or status");
+  BZ_REQUIRE(n >= 0 && limit > 0, "bz_field_check: need n >= 0 and limit > 0");
+  if (n == 0) return BZ_OK;
+  const int threads = 256;
+  const unsigned blocks = (unsigned)(bz::ceil_div(n, threads * 8) < 148 * 8 ? bz::ceil_div(n, threads * 8) : 148 * 8);
+  cudaStream_t st = bz::as_stream(stream);
+  if (dtype == BZ_F32)
+    field_check_kernel<float><<<blocks, threads, 0, st>>>((const float*)field, n, limit, step, (long long*)status);
+  else if (dtype == BZ_F64)
+    field_check_kernel<double><<<blocks, threads, 0, st>>>((const double*)field, n, limit, step, (long long*)status);
+  else
+    return bz::fail(BZ_ERR_INVALID, "bz_field_check: unknown dtype %d", dtype);
+  return bz::check_launch("bz_field_check");
+}

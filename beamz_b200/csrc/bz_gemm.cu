@@ -42,6 +42,8 @@ struct GemmP {
   long long ldc, sc;
   bf16* pre;
   long long ldpre, spre;
+  int wait_limit;  // polls of a bounded mbarrier wait before it gives up (tcgen05 kernel)
+  int withhold;    // 1: the tcgen05 kernel issues no MMA for its first K slice (timeout self-test)
 };
 
 __device__ __forceinline__ float gelu_f(float v) {
@@ -301,8 +303,8 @@ __device__ __forceinline__ uint64_t tc_sdesc(uint32_t saddr, uint32_t lbo, uint3
   return d;
 }
 
-__device__ __forceinline__ bool tc_wait(uint32_t mbar, uint32_t parity) {
-  for (int i = 0; i < tc::WAIT_LIMIT; ++i) {
+__device__ __forceinline__ bool tc_wait(uint32_t mbar, uint32_t parity, int limit = tc::WAIT_LIMIT) {
+  for (int i = 0; i < limit; ++i) {
     uint32_t ok;
     asm volatile(
         "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}\n"
@@ -385,7 +387,7 @@ __global__ void __launch_bounds__(tc::THREADS) gemm_tc_kernel(GemmP p) {
       const int s = (kt - kt0) & 1;
       asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
       __syncthreads();
-      if (tid == 0) {
+      if (tid == 0 && !(p.withhold && kt == kt0)) {
         asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
         const uint32_t a0 = sbase + s * tc::STAGE, b0 = a0 + tc::A_BYTES;
 #pragma unroll
@@ -407,7 +409,7 @@ __global__ void __launch_bounds__(tc::THREADS) gemm_tc_kernel(GemmP p) {
         gload(kt + 1);
         const int s2 = s ^ 1;
         if (kt > kt0) {  // the MMAs of the previous slice read stage s2
-          ok = tc_wait(mb0 + 8 * s2, phase[s2]);
+          ok = tc_wait(mb0 + 8 * s2, phase[s2], p.wait_limit);
           phase[s2] ^= 1u;
         }
         if (ok) sstore(s2);
@@ -415,9 +417,9 @@ __global__ void __launch_bounds__(tc::THREADS) gemm_tc_kernel(GemmP p) {
       ok = __syncthreads_and(ok);
     }
     if (ok) {
-      ok = tc_wait(mb0 + 8 * last, phase[last]);
-    } else {
-      tc_wait(mb0 + 8 * last, phase[last]);  // let issued MMAs drain before the TMEM goes
+      ok = tc_wait(mb0 + 8 * last, phase[last], p.wait_limit);
+    } else if (!(p.withhold && last == 0 && kt1 - kt0 == 1)) {
+      tc_wait(mb0 + 8 * last, phase[last], p.wait_limit);  // let issued MMAs drain before the TMEM goes
     }
     if (!ok && tid == 0) atomicExch(&g_tc_error, 1);
   }
@@ -897,6 +899,8 @@ extern "C" int bz_gemm_bf16(const bz_gemm* g, void* stream) {
   p.bias_m = g->bias_m; p.bias_n = g->bias_n;
   p.outf = g->outf; p.outh = (bz::bf16*)g->outh; p.ldc = g->ldc; p.sc = g->sc;
   p.pre = (bz::bf16*)g->pre; p.ldpre = g->ldpre; p.spre = g->spre;
+  p.wait_limit = bz::tc::WAIT_LIMIT;
+  p.withhold = 0;
   cudaStream_t st = bz::as_stream(stream);
   if (g->engine == 0 && bz::tc_eligible(p)) {
     const int t = bz::launch_gemm_tma(p, st);
@@ -907,6 +911,34 @@ extern "C" int bz_gemm_bf16(const bz_gemm* g, void* stream) {
   if (g->N <= 32) return bz::launch_gemm<128, 32, 4, 1>(p, st);
   if (g->M <= 32) return bz::launch_gemm<32, 128, 1, 4>(p, st);
   return bz::launch_gemm<128, 128, 2, 4>(p, st);
+}
+
+extern "C" int bz_gemm_wait_selftest(const void* A, const void* B, float* C, int32_t wait_limit, void* stream) {
+  BZ_REQUIRE(A && B && C, "bz_gemm_wait_selftest: NULL buffer");
+  BZ_REQUIRE(wait_limit >= 1, "bz_gemm_wait_selftest: wait_limit must be positive");
+  bz::GemmP p = {};
+  p.M = 128; p.N = 256; p.K = 64; p.batch = 1; p.splitk = 1;
+  p.A = (const bz::bf16*)A; p.lda = 64;
+  p.B = (const bz::bf16*)B; p.ldb = 64;
+  p.alpha = 1.0f;
+  p.outf = C; p.ldc = 256;
+  p.wait_limit = wait_limit;
+  p.withhold = 1;
+  cudaStream_t st = bz::as_stream(stream);
+  const int zero = 0;
+  if (cudaMemcpyToSymbolAsync(bz::g_tc_error, &zero, sizeof(int), 0, cudaMemcpyHostToDevice, st) != cudaSuccess)
+    return bz::fail(BZ_ERR_CUDA, "bz_gemm_wait_selftest: cannot reset the error word");
+  const int rc = bz::launch_gemm_tc(p, st);
+  if (rc != BZ_OK) return rc;
+  if (cudaStreamSynchronize(st) != cudaSuccess) return bz::fail(BZ_ERR_CUDA, "bz_gemm_wait_selftest: launch failed");
+  int v = 0;
+  if (cudaMemcpyFromSymbol(&v, bz::g_tc_error, sizeof(int)) != cudaSuccess)
+    return bz::fail(BZ_ERR_CUDA, "bz_gemm_wait_selftest: cannot read the error word");
+  if (cudaMemcpyToSymbol(bz::g_tc_error, &zero, sizeof(int)) != cudaSuccess)
+    return bz::fail(BZ_ERR_CUDA, "bz_gemm_wait_selftest: cannot reset the error word");
+  if (v) return bz::fail(BZ_ERR_TIMEOUT, "bz_gemm_wait_selftest: the withheld slice's wait ran out after %d polls",
+                         wait_limit);
+  return BZ_OK;
 }
 
 extern "C" int bz_gemm_error(int32_t* value, int32_t reset) {

@@ -14,7 +14,8 @@
 //   4. owned threads compute E(k) and write H(k), E(k).
 // The first plane's H(k-1) is recomputed from global memory. Ping-pong copies
 // keep every launch reading only the previous step's values. Float32 fields take
-// step3d_pair_kernel, the same schedule with two x cells per thread.
+// step3d_quad_kernel, the same schedule with four x cells per thread (float4), or on
+// request (bz_grid3d.x_cells = 2) step3d_pair_kernel with two.
 #include "bz_internal.cuh"
 
 namespace bz {
@@ -452,6 +453,242 @@ int launch3d_pair(const bz_grid3d* gd, const bz_fields3d* f, int64_t step, cudaS
   return check_launch("bz_step3d");
 }
 
+// ---------------------------------------------------------------------------- quad columns (float32)
+// The same schedule with four adjacent x cells per thread, moved as float4: a warp spans
+// 128 columns whose first four (one quad, to keep 16-byte alignment) are the halo shared
+// with the neighbouring tile, so a block owns 124 x (TY-1) columns. Against the pair
+// kernel, loads, stores, shared-memory traffic, shuffles and index arithmetic are issued
+// once per four cells. The quad starts at x % 4 == 0; cells past the last real column
+// (row padding, pitch % 32 == 0) are read as stored (zero) and never written, and no
+// written value depends on them.
+__device__ __forceinline__ float4 ld4(const float* p, long long i, bool ok) {
+  return ok ? __ldg(reinterpret_cast<const float4*>(p + i)) : make_float4(0.f, 0.f, 0.f, 0.f);
+}
+
+// Stores the first n (0..4) cells of a quad: one 16-byte store when all four exist.
+__device__ __forceinline__ void st4(float* p, long long i, float4 v, int n) {
+  if (n >= 4) {
+    *reinterpret_cast<float4*>(p + i) = v;
+    return;
+  }
+  if (n >= 1) p[i] = v.x;
+  if (n >= 2) p[i + 1] = v.y;
+  if (n >= 3) p[i + 2] = v.z;
+}
+
+__device__ __forceinline__ float& q_at(float4& v, int j) { return j == 0 ? v.x : (j == 1 ? v.y : (j == 2 ? v.z : v.w)); }
+__device__ __forceinline__ float q_get(const float4& v, int j) {
+  return j == 0 ? v.x : (j == 1 ? v.y : (j == 2 ? v.z : v.w));
+}
+
+struct QuadIn {
+  float4 hx, hy, hz, a, ce, ez_y, ex_y;
+  float ez_x, ey_x;  // E at x+4 (the warp's last lane)
+};
+
+// One column segment: tile (bx, by) of design/component dc, planes [z0, z1).
+template <int TY>
+__device__ __forceinline__ void quad_segment(const Ptr3<float>& in, const Out3<float>& out,
+                                             const float* __restrict__ ce, const float* __restrict__ loss,
+                                             const Geo3D<float>& g, int bx, int by, int dc, int z0, int z1,
+                                             float4 (*s_ez)[TX], float4 (*s_ex)[TX], float4 (*s_hz)[TX],
+                                             float4 (*s_hx)[TX]) {
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  const int nx = g.nx, ny = g.ny, nz = g.nz;
+  const int x = bx * (4 * TX - 4) - 4 + 4 * tx;  // first cell of the quad
+  const int y = by * (TY - 1) - 1 + ty;
+  const int d = dc / g.n_comp;
+  const bool xin = x >= 0 && x < nx, yin = y >= 0 && y < ny, inb = xin && yin;
+  const bool owned = inb && tx >= 1 && ty >= 1;
+  const bool xe = tx == TX - 1, ye = ty == TY - 1;
+  const bool xnb = yin && x + 4 < nx, ynb = xin && y + 1 < ny;
+  // cells of the quad inside each component's x extent (x <= nx-2 or x <= nx-1)
+  const int n_m = max(0, min(4, nx - 1 - x)), n_a = max(0, min(4, nx - x));
+  const bool yint = y >= 1 && y <= ny - 2, ym = y <= ny - 2;
+  const long long P = g.plane;
+  const long long mb = (g.n_mat > 1 ? (long long)d : 0LL) * g.vol;
+  const long long col = (long long)y * g.pitch + x;
+  const long long fb = (long long)dc * g.vol;
+
+  auto load_plane = [&](int k, QuadIn& q) {
+    const long long po = (long long)k * P + col;
+    q.a = ld4(loss + mb, po, inb);
+    q.ce = ld4(ce + mb, po, inb);
+    const long long o = fb + po;
+    q.hx = ld4(in.h[0], o, inb);
+    q.hy = ld4(in.h[1], o, inb);
+    q.hz = ld4(in.h[2], o, inb);
+    q.ez_x = ld(in.e[2], o + 4, xe && xnb);
+    q.ey_x = ld(in.e[1], o + 4, xe && xnb);
+    q.ez_y = ld4(in.e[2], o + g.pitch, ye && ynb);
+    q.ex_y = ld4(in.e[0], o + g.pitch, ye && ynb);
+  };
+
+  float4 exk, eyk, ezk, exn, eyn, ezn, hxm = make_float4(0.f, 0.f, 0.f, 0.f), hym = make_float4(0.f, 0.f, 0.f, 0.f);
+  QuadIn cur, nxt;
+  load_plane(z0, cur);
+  {
+    const long long o = fb + (long long)z0 * P + col;
+    exk = ld4(in.e[0], o, inb);
+    eyk = ld4(in.e[1], o, inb);
+    ezk = ld4(in.e[2], o, inb);
+    exn = ld4(in.e[0], o + P, inb && z0 + 1 < nz);
+    eyn = ld4(in.e[1], o + P, inb && z0 + 1 < nz);
+    ezn = ld4(in.e[2], o + P, inb && z0 + 1 < nz);
+  }
+  if (z0 >= 1 && inb) {  // Hx, Hy at plane z0-1 of the quad, recomputed from global memory
+    const long long po = (long long)(z0 - 1) * P + col, o = fb + po;
+    const float4 a = __ldg(reinterpret_cast<const float4*>(loss + mb + po));
+    const float4 ez = ld4(in.e[2], o, true), ex = ld4(in.e[0], o, true), ey = ld4(in.e[1], o, true);
+    const float4 ez_yp = ld4(in.e[2], o + g.pitch, y + 1 < ny);
+    const float ez_x4 = ld(in.e[2], o + 4, x + 4 < nx);
+    const float4 hx = ld4(in.h[0], o, true), hy = ld4(in.h[1], o, true);
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      float fh, cx, cy, cz;
+      hfac(q_get(a, j), g, fh, cx, cy, cz);
+      const float ez_xp = j < 3 ? q_get(ez, j + 1) : ez_x4;
+      q_at(hxm, j) = fh * q_get(hx, j) - (cy * (q_get(ez_yp, j) - q_get(ez, j)) - cz * (q_get(eyk, j) - q_get(ey, j)));
+      q_at(hym, j) = fh * q_get(hy, j) - (cz * (q_get(exk, j) - q_get(ex, j)) - cx * (ez_xp - q_get(ez, j)));
+    }
+  }
+
+  for (int k = z0; k < z1; ++k) {
+    const long long po = (long long)k * P + col;
+    float4 ex2, ey2, ez2;  // prefetch: inputs of plane k+1 and E(k+2)
+    if (k + 1 < z1) {
+      load_plane(k + 1, nxt);
+      const long long o = fb + po + 2 * P;
+      ex2 = ld4(in.e[0], o, inb && k + 2 < nz);
+      ey2 = ld4(in.e[1], o, inb && k + 2 < nz);
+      ez2 = ld4(in.e[2], o, inb && k + 2 < nz);
+    }
+    s_ez[ty][tx] = ezk;
+    s_ex[ty][tx] = exk;
+    __syncthreads();
+    const float4 ez_yp = ye ? cur.ez_y : s_ez[ty + (ye ? 0 : 1)][tx];
+    const float4 ex_yp = ye ? cur.ex_y : s_ex[ty + (ye ? 0 : 1)][tx];
+    float ez_x4 = __shfl_down_sync(FULL, ezk.x, 1);
+    float ey_x4 = __shfl_down_sync(FULL, eyk.x, 1);
+    if (xe) {
+      ez_x4 = cur.ez_x;
+      ey_x4 = cur.ey_x;
+    }
+    float4 hxn, hyn, hzn, fe4;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      float fh, cx, cy, cz;
+      hfac(q_get(cur.a, j), g, fh, cx, cy, cz);
+      const float ez_xp = j < 3 ? q_get(ezk, j + 1) : ez_x4;
+      const float ey_xp = j < 3 ? q_get(eyk, j + 1) : ey_x4;
+      const float ezc = q_get(ezk, j), eyc = q_get(eyk, j), exc = q_get(exk, j);
+      q_at(hxn, j) = fh * q_get(cur.hx, j) - (cy * (q_get(ez_yp, j) - ezc) - cz * (q_get(eyn, j) - eyc));
+      q_at(hyn, j) = fh * q_get(cur.hy, j) - (cz * (q_get(exn, j) - exc) - cx * (ez_xp - ezc));
+      q_at(hzn, j) = fh * q_get(cur.hz, j) - (cx * (ey_xp - eyc) - cy * (q_get(ex_yp, j) - exc));
+      q_at(fe4, j) = 1.f - q_get(cur.a, j) * q_get(cur.ce, j) * g.inv_kd2;
+    }
+    s_hz[ty][tx] = hzn;
+    s_hx[ty][tx] = hxn;
+    __syncthreads();
+    const float hy_xm = __shfl_up_sync(FULL, hyn.w, 1);
+    const float hz_xm = __shfl_up_sync(FULL, hzn.w, 1);
+    if (owned) {
+      const long long o = fb + po;
+      const float4 hz_ym = s_hz[ty - 1][tx];
+      const float4 hx_ym = s_hx[ty - 1][tx];
+      const bool kin = k >= 1 && k <= nz - 2, kz = k <= nz - 2;
+      float4 ex = exk, ey = eyk, ez = ezk;
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const bool xm = x + j <= nx - 2, xp = x + j >= 1;
+        const float cv = q_get(cur.ce, j), fe = q_get(fe4, j);
+        const float hzl = j > 0 ? q_get(hzn, j - 1) : hz_xm;
+        const float hyl = j > 0 ? q_get(hyn, j - 1) : hy_xm;
+        if (kin && yint && xm)
+          q_at(ex, j) = fe * q_get(exk, j) + cv * ((q_get(hzn, j) - q_get(hz_ym, j)) - g.qz * (q_get(hyn, j) - q_get(hym, j)));
+        if (kin && ym && xp && xm)
+          q_at(ey, j) = fe * q_get(eyk, j) + cv * (g.qz * (q_get(hxn, j) - q_get(hxm, j)) - g.qx * (q_get(hzn, j) - hzl));
+        if (kz && yint && xp && xm)
+          q_at(ez, j) = fe * q_get(ezk, j) + cv * (g.qx * (q_get(hyn, j) - hyl) - (q_get(hxn, j) - q_get(hx_ym, j)));
+      }
+      st4(out.e[0], o, ex, n_m);
+      st4(out.e[1], o, ey, ym ? n_a : 0);
+      st4(out.e[2], o, ez, kz ? n_a : 0);
+      st4(out.h[0], o, hxn, (kz && ym) ? n_a : 0);
+      st4(out.h[1], o, hyn, kz ? n_m : 0);
+      st4(out.h[2], o, hzn, ym ? n_m : 0);
+    }
+    exk = exn;
+    eyk = eyn;
+    ezk = ezn;
+    exn = ex2;
+    eyn = ey2;
+    ezn = ez2;
+    hxm = hxn;
+    hym = hyn;
+    cur = nxt;
+  }
+}
+
+// One block per (x tile, y tile, z block of ZB planes, design-component).
+template <int ZB, int TY>
+__global__ void __launch_bounds__(TX * TY, TY == 8 ? 2 : 1) step3d_quad_kernel(Ptr3<float> in, Out3<float> out,
+                                                                  const float* __restrict__ ce,
+                                                                  const float* __restrict__ loss,
+                                                                  Geo3D<float> g) {
+  __shared__ float4 s_ez[TY][TX], s_ex[TY][TX], s_hz[TY][TX], s_hx[TY][TX];
+  const int dc = blockIdx.z / g.nzb;
+  const int z0 = (blockIdx.z - dc * g.nzb) * ZB;
+  quad_segment<TY>(in, out, ce, loss, g, blockIdx.x, blockIdx.y, dc, z0, min(z0 + ZB, g.nz), s_ez, s_ex, s_hz, s_hx);
+}
+
+template <int TY>
+int launch3d_quad(const bz_grid3d* gd, const bz_fields3d* f, int64_t step, cudaStream_t st) {
+  Geo3D<float> g;
+  g.nx = gd->nx;
+  g.ny = gd->ny;
+  g.nz = gd->nz;
+  g.pitch = gd->pitch;
+  g.n_designs = gd->n_designs;
+  g.n_mat = gd->n_mat;
+  g.n_comp = gd->n_comp;
+  g.nzb = 1;
+  g.plane = (long long)gd->ny * gd->pitch;
+  g.vol = g.plane * gd->nz;
+  g.chx = (float)gd->chx;
+  g.chy = (float)gd->chy;
+  g.chz = (float)gd->chz;
+  g.qx = (float)gd->qx;
+  g.qz = (float)gd->qz;
+  g.inv_kd2 = (float)gd->inv_kd2;
+  const int src = (int)(step & 1);
+  Ptr3<float> in;
+  Out3<float> out;
+  for (int i = 0; i < 3; ++i) {
+    in.e[i] = (const float*)f->e[src][i];
+    in.h[i] = (const float*)f->h[src][i];
+    out.e[i] = (float*)f->e[src ^ 1][i];
+    out.h[i] = (float*)f->h[src ^ 1][i];
+  }
+  const int n_xt = (int)ceil_div(gd->nx, 4 * TX - 4), n_yt = (int)ceil_div(gd->ny, TY - 1);
+  dim3 block(TX, TY);
+  const int zb = gd->tile_z == 8 ? 8 : 16;
+  g.nzb = (int)ceil_div(gd->nz, zb);
+  dim3 grid((unsigned)n_xt, (unsigned)n_yt, (unsigned)(g.nzb * gd->n_designs * gd->n_comp));
+  if (zb == 8)
+    step3d_quad_kernel<8, TY><<<grid, block, 0, st>>>(in, out, (const float*)f->ce, (const float*)f->loss, g);
+  else
+    step3d_quad_kernel<16, TY><<<grid, block, 0, st>>>(in, out, (const float*)f->ce, (const float*)f->loss, g);
+  return check_launch("bz_step3d");
+}
+
+inline bool vec_aligned(const bz_fields3d* f, uintptr_t bytes) {
+  bool ok = ((uintptr_t)f->ce | (uintptr_t)f->loss) % bytes == 0;
+  for (int c = 0; c < 2; ++c)
+    for (int i = 0; i < 3; ++i) ok = ok && ((uintptr_t)f->e[c][i] | (uintptr_t)f->h[c][i]) % bytes == 0;
+  return ok;
+}
+
 // float2 accesses need every array 8-byte aligned (offsets are even: pitch % 32 == 0).
 inline bool pair_aligned(const bz_fields3d* f) {
   bool ok = ((uintptr_t)f->ce | (uintptr_t)f->loss) % 8 == 0;
@@ -462,14 +699,18 @@ inline bool pair_aligned(const bz_fields3d* f) {
 
 template <typename T, int TY>
 int dispatch3d_ty(const bz_grid3d* g, const bz_fields3d* f, int64_t step, cudaStream_t st) {
-  const bool z8 = g->tile_z == 8;
+  const bool z8 = g->tile_z == 8;  // 0 takes 16-plane z blocks
   if (g->n_comp == 1) return z8 ? launch3d<T, 1, 8, TY>(g, f, step, st) : launch3d<T, 1, 16, TY>(g, f, step, st);
   return z8 ? launch3d<T, 2, 8, TY>(g, f, step, st) : launch3d<T, 2, 16, TY>(g, f, step, st);
 }
 
 template <typename T>
 int dispatch3d(const bz_grid3d* g, const bz_fields3d* f, int64_t step, cudaStream_t st) {
-  if (sizeof(T) == 4 && pair_aligned(f) && (long long)g->n_designs * g->n_comp * ceil_div(g->nz, 8) <= 65535) {
+  const bool zfit = (long long)g->n_designs * g->n_comp * ceil_div(g->nz, 8) <= 65535;
+  if (sizeof(T) == 4 && (g->x_cells == 0 || g->x_cells == 4) && vec_aligned(f, 16) && zfit) {
+    return g->tile_y == 16 ? launch3d_quad<16>(g, f, step, st) : launch3d_quad<8>(g, f, step, st);
+  }
+  if (sizeof(T) == 4 && g->x_cells != 1 && pair_aligned(f) && zfit) {
     const bool z8 = g->tile_z == 8;
     if (g->tile_y == 16) return z8 ? launch3d_pair<8, 16>(g, f, step, st) : launch3d_pair<16, 16>(g, f, step, st);
     return z8 ? launch3d_pair<8, 8>(g, f, step, st) : launch3d_pair<16, 8>(g, f, step, st);
@@ -564,6 +805,8 @@ extern "C" int bz_step3d(const bz_grid3d* g, const bz_fields3d* f, int64_t step,
   BZ_REQUIRE(g->n_mat == 1 || g->n_mat == g->n_designs, "bz_step3d: n_mat must be 1 or n_designs");
   BZ_REQUIRE(g->tile_z == 0 || g->tile_z == 8 || g->tile_z == 16, "bz_step3d: tile_z must be 0, 8 or 16");
   BZ_REQUIRE(g->tile_y == 0 || g->tile_y == 8 || g->tile_y == 16, "bz_step3d: tile_y must be 0, 8 or 16");
+  BZ_REQUIRE(g->x_cells == 0 || g->x_cells == 1 || g->x_cells == 2 || g->x_cells == 4,
+             "bz_step3d: x_cells must be 0, 1, 2 or 4");
   for (int c = 0; c < 2; ++c)
     for (int i = 0; i < 3; ++i) BZ_REQUIRE(f->e[c][i] && f->h[c][i], "bz_step3d: field buffer is NULL");
   BZ_REQUIRE(f->ce && f->loss, "bz_step3d: coefficient arrays are NULL");

@@ -18,6 +18,7 @@ from .. import _native as nat
 from ..const import EPS_0, MU_0
 from .compile_ops import SourceOps, compile_monitors_2d, compile_sources
 from .graphs import capture, dft_phasors
+from .guard import DivergenceGuard
 
 GRAPH_CHUNK = 64  # at most this many steps per captured graph
 RING_LEN = GRAPH_CHUNK  # monitor samples kept between DFT folds
@@ -85,6 +86,7 @@ class Engine2D:
         # steps per graph: an even number of steps keeps the copy parity, so one
         # graph serves every chunk of a run
         self.chunk = GRAPH_CHUNK // (2 * self.time_block) * (2 * self.time_block)
+        self.guard = DivergenceGuard(self.dev, every=8 * self.chunk)  # checks fall on chunk boundaries
         self.n_step_launches = 0  # step-kernel launches issued (graph nodes included)
         self.n_fold_launches = 0
         g = nat.Grid2D()
@@ -270,6 +272,7 @@ class Engine2D:
                 t.zero_()
         self.step_index = 0
         self._folded = 0
+        self.guard.reset()
         if self.record is not None:
             self._rec_host = []
             self.mops.rec_step0 = 0
@@ -319,11 +322,28 @@ class Engine2D:
             self.tune_times = times
         self.time_block, self.tb_tile = _TUNED[key]
         self.chunk = GRAPH_CHUNK // (2 * self.time_block) * (2 * self.time_block)
+        self.guard.every = 8 * self.chunk  # checks fall on chunk boundaries
+        self.guard.next = (self.step_index // self.guard.every + 1) * self.guard.every
         self._graphs.clear()
         self._autotune = False
         return _TUNED[key]
 
     def run_steps(self, n: int):
+        """Advance n steps (see _run_steps); the E field is scanned for divergence every
+        guard.every steps."""
+        while n > 0:
+            k = min(n, max(1, self.guard.next - self.step_index))
+            self._run_steps(k)
+            n -= k
+            self.guard.maybe_check(self.ez[self.cur], self.bz_dtype, self.step_index)
+
+    def check_divergence(self):
+        """Scan the current E field and raise NativeError(BZ_ERR_DIVERGED) if this run
+        diverged at any check so far (synchronizes)."""
+        self.guard.check(self.ez[self.cur], self.bz_dtype, self.step_index)
+        self.guard.raise_if_diverged()
+
+    def _run_steps(self, n: int):
         """Advance n steps, replaying graph chunks where the record buffer allows."""
         if self._autotune:
             self.autotune()

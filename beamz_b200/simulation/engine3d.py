@@ -17,6 +17,7 @@ from ..const import EPS_0, MU_0
 from ..devices.monitors import Monitor
 from .compile_ops import compile_sources
 from .graphs import capture, dft_phasors
+from .guard import DivergenceGuard
 
 GRAPH_CHUNK = 32
 RING_LEN = GRAPH_CHUNK
@@ -29,7 +30,7 @@ def _round_up(n, m):
 
 class Engine3D:
     def __init__(self, eps_r, sigma, dx, dy, dz, dt, n_steps, sources, monitors, *, precision="fp32", n_comp=None,
-                 power=False, n_designs=1, record=True, use_graphs=True, tile_z=16, tile_y=8, device=None):
+                 power=False, n_designs=1, record=True, use_graphs=True, tile_z=0, tile_y=8, x_cells=0, device=None):
         if not torch.cuda.is_available():
             raise RuntimeError("beamz_b200 needs a CUDA GPU (sm_100a); none is visible")
         self.dev = torch.device("cuda", torch.cuda.current_device()) if device is None else torch.device(device)
@@ -69,6 +70,7 @@ class Engine3D:
         g.nx, g.ny, g.nz, g.pitch = self.nx, self.ny, self.nz, self.pitch
         g.n_designs, g.n_comp, g.n_mat, g.dtype, g.tile_z = n_designs, self.n_comp, self.n_mat, self.bz_dtype, tile_z
         g.tile_y = int(tile_y)
+        g.x_cells = int(x_cells)
         g.chx, g.chy, g.chz = self.dt / (MU_0 * self.dx), self.dt / (MU_0 * self.dy), self.dt / (MU_0 * self.dz)
         g.qx, g.qz = self.dy / self.dx, self.dy / self.dz
         g.inv_kd2 = 2.0 * EPS_0 * self.dy / self.dt
@@ -81,6 +83,7 @@ class Engine3D:
         self.use_graphs = use_graphs
         self._graphs = {}
         self.kernel_timer = None  # graphs.KernelTimer around the step launches (direct launches only)
+        self.guard = DivergenceGuard(self.dev)
         # kernels per step: the step itself, source operations, monitor gather, power
         self.kernels_per_step = 1 + (self.sops.n_ops > 0) + (self.gops is not None) + (self.power is not None)
         self.n_step_launches = 0  # bz_step3d launches (one per step, graph nodes included)
@@ -218,6 +221,21 @@ class Engine3D:
         return g
 
     def run_steps(self, n):
+        """Advance n steps (see _run_steps); the E field is scanned for divergence every
+        guard.every steps."""
+        while n > 0:
+            k = min(n, max(1, self.guard.next - self.step_index))
+            self._run_steps(k)
+            n -= k
+            self.guard.maybe_check(self.f["Ez"][self.cur], self.bz_dtype, self.step_index)
+
+    def check_divergence(self):
+        """Scan the current E field and raise NativeError(BZ_ERR_DIVERGED) if this run
+        diverged at any check so far (synchronizes)."""
+        self.guard.check(self.f["Ez"][self.cur], self.bz_dtype, self.step_index)
+        self.guard.raise_if_diverged()
+
+    def _run_steps(self, n):
         while n > 0:
             self._maybe_drain()
             room = n
@@ -259,6 +277,7 @@ class Engine3D:
                 t.zero_()
         self.step_index = 0
         self._folded = 0
+        self.guard.reset()
         if self.record is not None:
             self._rec_host = []
             self.gops.rec_step0 = 0

@@ -113,7 +113,8 @@ class FDTD:
             self.engine = Engine3D(self.mesh.permittivity, self.mesh.conductivity, self.dx, self.dy, self.dz,
                                    self.dt, self.num_steps, self.sources, self.monitors, precision=precision,
                                    n_comp=n_comp, power=accumulate_power, use_graphs=graphs,
-                                   tile_z=opts.get("tile_z", 16), tile_y=opts.get("tile_y", 8))
+                                   tile_z=opts.get("tile_z", 0), tile_y=opts.get("tile_y", 8),
+                                   x_cells=opts.get("x_cells", 0))
         else:
             from .engine2d import Engine2D
 
@@ -292,6 +293,9 @@ class FDTD:
 
     def finalize_simulation(self):
         if self.engine is not None:
+            # raises NativeError(BZ_ERR_DIVERGED) if the fields ran away (the reference
+            # only warns about the Courant number before the run, fdtd.py:375-383)
+            self.engine.check_divergence()
             self._collect_monitors()
             if self.accumulate_power:
                 pm = self.engine.power_map()

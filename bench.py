@@ -55,7 +55,11 @@ def parse():
     p.add_argument("--nz", type=int, default=None, help="soi_mmi_3d: z planes (default 150; smaller for profiling)")
     p.add_argument("--cpu-steps", type=int, default=60, help="time steps of the CPU baseline sample")
     p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline sample (A/B and profiling runs)")
     p.add_argument("--n-comp", type=int, default=1, help="field components: 1 = real (physical) field, 2 = Re+Im")
+    p.add_argument("--x-cells", type=int, default=0, help="3D: x cells per thread (0 = the library's choice)")
+    p.add_argument("--tile-y", type=int, default=8, help="3D: rows per thread block (8 or 16)")
+    p.add_argument("--tile-z", type=int, default=16, help="3D: z planes per thread block (8 or 16)")
     return p.parse_args()
 
 
@@ -227,7 +231,8 @@ def run_b200(args):
     shape = grid.permittivity.shape
     cells = int(np.prod(shape))
     n_steps = len(t)
-    sim = FDTD(design=grid, time=t, backend_options={"n_comp": args.n_comp})
+    opts = {"n_comp": args.n_comp, "x_cells": args.x_cells, "tile_y": args.tile_y, "tile_z": args.tile_z}
+    sim = FDTD(design=grid, time=t, backend_options=opts)
     sim.initialize_simulation(save=False, live=False, save_memory_mode=True)
     eng = sim.engine
     flush = torch.empty(512 << 20, dtype=torch.uint8, device="cuda")
@@ -243,7 +248,8 @@ def run_b200(args):
         if evs is not None:
             evs[1].record()
 
-    count = (lambda: eng.n_kernel_launches) if is3d else (lambda: eng.n_step_launches + eng.n_fold_launches)
+    count = (lambda: eng.n_kernel_launches + eng.guard.launches) if is3d else \
+        (lambda: eng.n_step_launches + eng.n_fold_launches + eng.guard.launches)
     l0, k0 = eng.n_step_launches, count()
     one_run()  # the 2D engine picks its launch shape here (autotuner)
     step_launches, all_launches = eng.n_step_launches - l0, count() - k0
@@ -275,6 +281,7 @@ def run_b200(args):
         dist.barrier()
     ck = clocks.stop()
     eng.kernel_timer = None
+    eng.check_divergence()
     total_ms = t_start.elapsed_time(t_end)
     kern_ms = timer.durations_ms()
     total_ms = max_over_ranks(total_ms, world, "cuda")
@@ -296,7 +303,7 @@ def run_b200(args):
         e2e = run_e2e(grid, t, cells, n_steps, args, world)
 
     cpu = None
-    if rank == 0 and world == 1:
+    if rank == 0 and world == 1 and not args.no_cpu:
         d._bench_eps, d._bench_sigma = grid.permittivity, grid.conductivity
         ncpu = min(args.cpu_steps if not is3d else 2, n_steps)
         v, el = cpu_baseline(d, t, dx, ncpu)
@@ -337,7 +344,9 @@ def run_b200(args):
             line["roofline"]["note"] = (f"{kname}: one time step per launch x {cell_bytes} B/cell (six fields read "
                                         f"and written, ce and loss read) x {cells} cells; {timing}; peak "
                                         f"{peak_kind} copy bandwidth; traffic {traffic_note}")
-            line["tile"] = "paired columns: 32 x 8 threads x 2 cells, 16-plane z blocks"
+            xc = args.x_cells or 4
+            line["tile"] = (f"32 x {args.tile_y} threads x {xc} x cells ({32 * xc - xc} x {args.tile_y - 1} owned "
+                            f"columns), {args.tile_z or 16}-plane z blocks")
         else:
             line["roofline"]["note"] = (f"{kname}: {tb} time steps per launch x {cell_bytes} B/cell (algorithmic, "
                                         f"one-step) x {cells} cells; {timing}; peak {peak_kind} copy bandwidth; "
@@ -368,7 +377,8 @@ def run_e2e(grid, t, cells, n_steps, args, world):
     for k in range(max(1, min(args.steps, 3))):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        sim = FDTD(design=grid, time=t, backend_options={"n_comp": args.n_comp})
+        sim = FDTD(design=grid, time=t, backend_options={"n_comp": args.n_comp, "x_cells": args.x_cells,
+                                                         "tile_y": args.tile_y, "tile_z": args.tile_z})
         sim.run(live=False, save=False, save_memory_mode=True)
         torch.cuda.synchronize()
         times.append(time.perf_counter() - t0)

@@ -265,6 +265,8 @@ typedef struct bz_grid3d {
   int32_t n_designs, n_comp, n_mat, dtype;
   int32_t tile_z;           /* z planes per thread block: 8 or 16 (0 = 16) */
   int32_t tile_y;           /* rows per thread block (32 x tile_y threads): 8 or 16 (0 = 8) */
+  int32_t x_cells;          /* x cells per thread for float32 fields: 4, 2 or 1 (0 = 4);
+                               float64 fields always take 1 */
   double chx, chy, chz, qx, qz, inv_kd2;
 } bz_grid3d;
 
@@ -315,6 +317,15 @@ int bz_power3d(const bz_grid3d* g, const bz_fields3d* f, int32_t cur, double* po
 int bz_dft_fold_q(const void* ring, int32_t dtype, int32_t ring_len, int64_t n_items, int32_t n_q, int32_t n_e,
                   int32_t n_freq, const double* phasor, int64_t n_phasor, int64_t step0, int32_t count, double* dft,
                   void* stream);
+
+/* Divergence guard (the reference only warns about the Courant number before a run,
+ * fdtd.py:375-383, helpers.py:21-53; this checks the fields while they run): scans n
+ * values of a field array and, when one is not finite or exceeds `limit` in magnitude,
+ * stores BZ_ERR_DIVERGED in status[0] and `step` in status[1] (device int64 words,
+ * zeroed by the caller; an earlier detection is kept). Asynchronous: the caller reads
+ * the words when it synchronizes and reports BZ_ERR_DIVERGED. */
+int bz_field_check(const void* field, int32_t dtype, int64_t n, double limit, int64_t step, int64_t* status,
+                   void* stream);
 
 /* ----------------------------------------------------------------------------
  * Rasteriser (meshing.py:92-536): painter's-order supersampled blend of each
@@ -431,6 +442,16 @@ int bz_gemm_bf16(const bz_gemm* g, void* stream);
 /* Error word of the tcgen05 GEMM (non-zero: a pipeline wait ran out; that CTA left
  * its tile unwritten). Synchronous read; reset = 1 clears it. */
 int bz_gemm_error(int32_t* value, int32_t reset);
+
+/* Drives the tcgen05 GEMM's bounded-wait error path on one 128 x 256 x 64 tile (no
+ * counterpart in the reference, which has no device code: this checks that a wait that
+ * never completes ends the kernel cleanly). The control thread issues no MMA for the
+ * tile's only K slice, so the wait for that slice's commit gives up after wait_limit
+ * polls; the kernel skips its epilogue, frees its tensor memory and raises the error
+ * word, which this call reads and clears. A: 128 x 64 bf16, B: 256 x 64 bf16 (row
+ * major, K contiguous), C: 128 x 256 f32 (not written). Synchronizes the stream.
+ * Returns BZ_ERR_TIMEOUT when the wait ran out, BZ_OK if the word stayed clear. */
+int bz_gemm_wait_selftest(const void* A, const void* B, float* C, int32_t wait_limit, void* stream);
 
 /* Spectral channel mixing of one Fourier layer, per mode k < n_modes:
  * O[b][o][k] = sum_c U[b][c][k] * W[k][c][o] (complex, (re, im) pairs, bf16);

@@ -145,16 +145,23 @@ def test_step3d_odd_grid_complex_vs_oracle(bz, precision, tol, tile_y):
     assert np.abs(got - want).max() <= tol * np.abs(want).max()
 
 
-@pytest.mark.parametrize("shape", [(9, 11, 13), (12, 17, 131), (10, 9, 128)])
-@pytest.mark.parametrize("tile_z,tile_y", [(16, 8), (8, 8), (16, 16), (8, 16)])
-def test_step3d_real_fp32_vs_oracle(bz, shape, tile_z, tile_y):
-    """Real float32 fields (stepped two x cells per thread): odd nx (the last pair ends in
-    row padding), several x tiles (62 owned columns each), several z blocks."""
+@pytest.mark.parametrize("x_cells", [4, 2, 1])
+@pytest.mark.parametrize("shape", [(9, 11, 13), (12, 17, 131), (10, 9, 128), (7, 10, 250), (37, 23, 70)])
+@pytest.mark.parametrize("tile_z,tile_y", [(0, 8), (16, 8), (8, 8), (0, 16), (16, 16), (8, 16)])
+def test_step3d_real_fp32_vs_oracle(bz, shape, tile_z, tile_y, x_cells):
+    """Real float32 fields stepped four, two or one x cells per thread: nx not a multiple
+    of the cells per thread (the last group ends in row padding), several x tiles (124 or
+    62 owned columns each), several z blocks (tile_z 0 is the default, 16)."""
+    if x_cells == 1 and (tile_z, tile_y) != (16, 8):
+        pytest.skip("one layout is enough for the scalar kernel")
+    if x_cells == 2 and tile_z == 0:
+        pytest.skip("the same layout as tile_z 16")
     d, grid, eps, sig, dx, dt, t, _, sgn = _odd_problem(bz, shape=shape)
     nz, ny, nx = shape
     g = bz.GaussianSource(position=((nx - 3) * dx, 5 * dx, 4 * dx), width=dx / 10, signal=sgn)
     g2 = bz.GaussianSource(position=(2 * dx, (ny - 3) * dx, (nz - 4) * dx), width=dx / 10, signal=sgn)
-    sim = bz.FDTD(design=grid, time=t, backend_options={"precision": "fp32", "tile_z": tile_z, "tile_y": tile_y})
+    sim = bz.FDTD(design=grid, time=t, backend_options={"precision": "fp32", "tile_z": tile_z, "tile_y": tile_y,
+                                                        "x_cells": x_cells})
     sim.sources = [g, g2]
     sim.run(live=False, save=False, save_memory_mode=True)
     assert sim.engine.n_comp == 1
