@@ -18,9 +18,12 @@
 // call before the fold reads it. Calls that overlap on the GPU (on different streams,
 // or from different host threads) race on the ring.
 //
-// Set-up: host code cannot use the array's name as a device address. So the first
-// call on each device, with that device current, looks the address up with
-// cudaGetSymbolAddress and keeps it. Make that first call before any stream capture.
+// Set-up: host code cannot use the array's name as a device address. So every call
+// made outside a stream capture looks the address up with cudaGetSymbolAddress, with
+// the device current, and keeps it per device ordinal; a call made while its stream is
+// being captured uses the kept address (a lookup can load the module, which a capture
+// does not allow). Make the first call on each device before any stream capture. A
+// device reset between a capture and its replay leaves the captured address stale.
 #include <mutex>
 
 #include "bz_internal.cuh"
@@ -35,15 +38,24 @@ constexpr int kMaxDevices = 64;
 void* g_ring_addr[kMaxDevices] = {};
 std::mutex g_ring_mu;
 
-// Device address of g_static_ring on the current device (looked up once per device).
-int static_ring_address(void** out) {
+// Device address of g_static_ring on the current device: looked up on every call
+// outside a capture (so a new context after a device reset gets its own address), the
+// kept one during a capture.
+int static_ring_address(cudaStream_t stream, void** out) {
   int dev = -1;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return bz::fail(BZ_ERR_CUDA, "bz_step2d_dft_static: cudaGetDevice: %s", cudaGetErrorString(e));
   if (dev < 0 || dev >= kMaxDevices)
     return bz::fail(BZ_ERR_UNSUPPORTED, "bz_step2d_dft_static: device ordinal %d is not below %d", dev, kMaxDevices);
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  e = cudaStreamIsCapturing(stream, &cap);
+  if (e != cudaSuccess)
+    return bz::fail(BZ_ERR_CUDA, "bz_step2d_dft_static: cudaStreamIsCapturing: %s", cudaGetErrorString(e));
   std::lock_guard<std::mutex> lock(g_ring_mu);
-  if (g_ring_addr[dev] == nullptr) {
+  if (cap == cudaStreamCaptureStatusNone || g_ring_addr[dev] == nullptr) {
+    if (cap != cudaStreamCaptureStatusNone)
+      return bz::fail(BZ_ERR_INVALID, "bz_step2d_dft_static: the first call on device %d is inside a stream "
+                      "capture; call it once before capturing", dev);
     void* p = nullptr;
     e = cudaGetSymbolAddress(&p, g_static_ring);
     if (e != cudaSuccess || p == nullptr)
@@ -77,7 +89,7 @@ extern "C" int bz_step2d_dft_static(const bz_grid2d* g, const bz_fields2d* f, co
   unsigned long long fit = BZ_STATIC_RING_BYTES / step_bytes;
   const int ring_len = (int)(fit < 64ull ? fit : 64ull);
   void* ring = nullptr;
-  int st = static_ring_address(&ring);
+  int st = static_ring_address(bz::as_stream(stream), &ring);
   if (st != BZ_OK) return st;
   bz_monitor_ops m = *mon;
   m.ring = ring;

@@ -180,9 +180,10 @@ int bz_dft_fold(const void* ring, int32_t dtype, int32_t ring_len, int64_t n_ite
  * dft ([n_designs*n_comp*n_points][n_freq][5][2], float64) exactly as bz_dft_fold does,
  * keeping the sample ring in an 8 MiB array compiled into the library instead of
  * mon->ring, which must be NULL. One step of samples (n_designs*n_comp*n_points*5
- * elements of dtype) must fit in 8 MiB; larger requests return BZ_ERR_INVALID. The
- * first call on a device looks up the array's address (make it before any stream
- * capture). All calls share the array; calls that overlap on the GPU race. */
+ * elements of dtype) must fit in 8 MiB; larger requests return BZ_ERR_INVALID. Calls
+ * outside a stream capture look up the array's address on the current device; make the
+ * first call on each device before any stream capture. All calls share the array;
+ * calls that overlap on the GPU race. */
 int bz_step2d_dft_static(const bz_grid2d* g, const bz_fields2d* f, const bz_source_ops* src,
                          const bz_monitor_ops* mon, int64_t step0, int32_t n_steps, int32_t n_freq,
                          const double* phasor, int64_t n_phasor, double* dft, void* stream);

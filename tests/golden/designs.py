@@ -9,6 +9,9 @@ from __future__ import annotations
 
 import numpy as np
 
+from pathlib import Path
+
+HERE = Path(__file__).resolve().parent
 UM = 1e-6
 RES = 0.05 * UM  # 50 nm cells keep the fixtures small
 
@@ -36,6 +39,22 @@ def raster_shapes(bz):
     for b in d.boundaries:
         b.polynomial_order = 3
         b.sigma_factor = 1.151
+    return d
+
+
+def raster_custom(bz):
+    """CustomMaterial on the rectangle path: a function-defined permittivity and
+    conductivity, and a grid-defined permittivity interpolated over its bounds, next to a
+    plain rectangle; default automatic PML."""
+    d = bz.Design(width=2.51 * UM, height=2.02 * UM, material=bz.Material(2.085), pml_size=0.3 * UM)
+    f = bz.CustomMaterial(permittivity_func=lambda x, y, z=0: 2.0 + 1.5 * np.sin(x / (0.31 * UM)) ** 2
+                          + 0.7 * np.cos(y / (0.17 * UM)),
+                          conductivity_func=lambda x, y, z=0: 50.0 * (x / UM) * (y / UM))
+    d += bz.Rectangle(position=(0.42 * UM, 0.37 * UM), width=0.93 * UM, height=0.61 * UM, material=f)
+    grid = 3.0 + np.add.outer(np.linspace(0.0, 2.0, 7), np.linspace(0.0, 5.0, 9))
+    g = bz.CustomMaterial(permittivity_grid=grid, bounds=((1.2 * UM, 2.1 * UM), (1.0 * UM, 1.7 * UM)))
+    d += bz.Rectangle(position=(1.18 * UM, 0.97 * UM), width=0.96 * UM, height=0.77 * UM, material=g)
+    d += bz.Rectangle(position=(0.2 * UM, 1.5 * UM), width=0.7 * UM, height=0.21 * UM, material=bz.Material(9.0))
     return d
 
 

@@ -17,6 +17,13 @@ simulation path), and its own NumPy backend (float64 / complex128) produces:
 * raster3d.npz   RegularGrid3D output (the reference's own 3D rasteriser)
 * step3d.npz     final six field components, z-normal plane monitor records and
                  accumulated power of a short 3D run on prescribed eps/sigma
+* raster_custom.npz  RegularGrid output for CustomMaterial rectangles (function- and
+                 grid-defined properties)
+* monitor_saved.npz  a line monitor's recorded fields and power written by the
+                 reference's own Monitor.save_data after a short 2D run
+
+``--only name1,name2`` regenerates just those fixtures (the mode-source runs depend on
+ARPACK's random start vector, so a full regeneration changes their files).
 
 The tests rebuild the same designs through beamz_b200 (``designs.py``) and compare.
 """
@@ -129,8 +136,34 @@ def step3d_run(bz, n_steps=60):
     return d, grid, t, [g, m], [mz, mx]
 
 
-def main(ref_path: str):
+def custom_fixture(bz):
+    g = bz.RegularGrid(D.raster_custom(bz), D.RES)
+    np.savez_compressed(HERE / "raster_custom.npz", eps=g.permittivity, mu=g.permeability, sigma=g.conductivity)
+
+
+def monitor_saved_fixture(bz):
+    """A short Gaussian-source run with one recording line monitor (power on), saved by
+    the reference's Monitor.save_data."""
+    d = D.wg_design(bz)
+    t = D.time_axis(bz, 40)
+    d += bz.GaussianSource(position=(1.0 * D.UM, 1.0 * D.UM), width=0.1 * D.UM, signal=D.gauss_signal(bz, t))
+    mon = bz.Monitor(design=d, start=(1.6 * D.UM, 0.6 * D.UM), end=(1.6 * D.UM, 1.4 * D.UM), name="m",
+                     record_interval=2)
+    d += mon
+    sim = bz.FDTD(design=bz.RegularGrid(d, D.RES), time=t)
+    sim.run(live=False, save=False, save_memory_mode=True)
+    mon.save_data(str(HERE / "monitor_saved.npz"))
+
+
+def main(ref_path: str, only=None):
     bz = import_reference(ref_path)
+    if only:
+        for name in only:
+            {"raster_custom": custom_fixture, "monitor_saved": monitor_saved_fixture}[name](bz)
+        print("fixtures written to", HERE)
+        return
+    custom_fixture(bz)
+    monitor_saved_fixture(bz)
     for name, builder in (("shapes", D.raster_shapes), ("pml_only", D.raster_pml_only)):
         g = bz.RegularGrid(builder(bz), D.RES)
         np.savez_compressed(HERE / f"raster_{name}.npz", eps=g.permittivity, mu=g.permeability, sigma=g.conductivity)
@@ -181,4 +214,10 @@ def main(ref_path: str):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    import argparse
+
+    ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
+    ap.add_argument("reference", help="path of the reference beamz source tree")
+    ap.add_argument("--only", default="", help="comma-separated fixture names (raster_custom, monitor_saved)")
+    a = ap.parse_args()
+    main(a.reference, [n for n in a.only.split(",") if n])

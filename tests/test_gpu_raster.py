@@ -26,3 +26,15 @@ def test_rasterizer_shapes_nontrivial(bz):
     grid = bz.RegularGrid(D.raster_shapes(bz), D.RES)
     assert len(np.unique(grid.permittivity)) > 30
     assert (grid.conductivity > 0).sum() > 500
+
+
+def test_custom_material_raster_bit_exact(bz, golden):
+    """CustomMaterial rectangles (function- and grid-defined properties) against the
+    reference's RegularGrid output."""
+    import designs as D
+
+    g = golden("raster_custom")
+    grid = bz.RegularGrid(D.raster_custom(bz), D.RES)
+    np.testing.assert_array_equal(grid.permittivity, g["eps"])
+    np.testing.assert_array_equal(grid.permeability, g["mu"])
+    np.testing.assert_array_equal(grid.conductivity, g["sigma"])
