@@ -220,7 +220,7 @@ class Engine2D:
     def _launch_tb(self, step_arg: int, d_step_ptr):
         timer = self.kernel_timer
         if timer is not None:
-            timer.before()
+            timer.before(self.time_block)
         nat.step2d_multi(self.grid, self._fields(), self.sops if self.sops.n_ops else None,
                          self.mops if self.mops.n_points else None, step_arg, self.time_block, self.tb_tile,
                          d_step_ptr, self._stream())

@@ -39,14 +39,16 @@ class KernelTimer:
         self.every = max(1, int(every))
         self.pairs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
                       for _ in range(capacity)]
+        self.steps = []  # time steps advanced by each timed launch
         self.n_launch = 0
         self.used = 0
         self._open = False
 
-    def before(self):
+    def before(self, steps: int = 1):
         self._open = self.n_launch % self.every == 0 and self.used < len(self.pairs)
         if self._open:
             self.pairs[self.used][0].record()
+            self.steps.append(int(steps))
 
     def after(self):
         if self._open:

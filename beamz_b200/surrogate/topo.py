@@ -204,11 +204,36 @@ def plain_adjoint(problem: TransmissionProblem, rho0: np.ndarray, iterations: in
 
 
 class SurrogateSearch:
+    """Surrogate-ranked ascent of the mean transmission, every accepted design judged by
+    a batched FDTD forward run.
+
+    Round r, from the current design rho and its exact adjoint gradient g (when the last
+    round fell back) or the surrogate's own input gradient (when it did not):
+      1. candidates: steps of a geometric ladder of sizes along the ascent directions
+         (the exact gradient, the surrogate's gradient and mixes of the two, each scaled
+         to a unit peak), and smooth random perturbations of the best-predicted ones;
+         each is box-blurred (radius 1) and clipped to [0, 1] as a plain ascent step is;
+      2. verification: ``n_anchor`` steps along the exact gradient at fixed sizes (when
+         it is known) plus the ``n_verify - n_anchor`` candidates the surrogate ranks
+         highest, in one batched FDTD forward; with ``use_surrogate=False`` the whole
+         batch is evenly spaced ladder steps along the exact gradient (the method
+         without the network);
+      3. the best verified design replaces rho when it raises the verified T;
+      4. fallback: when the surrogate misses a verified T by more than ``tol`` (or no
+         candidate improved), the next round's direction is the exact adjoint gradient
+         at rho (a plain per-design adjoint run); otherwise it is the surrogate's own;
+      5. the verified samples fine-tune the surrogate (mixed with training samples).
+    ``log`` keeps, per round, the best T, the surrogate's largest miss and whether it
+    fell back."""
+
     def __init__(self, problem: TransmissionProblem, net: FNO2d, n_candidates=256, n_verify=16, tol=1e-2,
-                 adjoint_step=0.05, seed=0, replay=None):
+                 adjoint_step=0.05, seed=0, replay=None, use_surrogate=True, n_anchor=4, ladder=(0.01, 0.8)):
         self.problem, self.net = problem, net
         self.n_cand, self.n_verify, self.tol = n_candidates, n_verify, tol
         self.adjoint_step = adjoint_step
+        self.use_surrogate = use_surrogate
+        self.n_anchor = min(n_anchor, n_verify // 2)
+        self.ladder = ladder
         self.gen = torch.Generator(device=net.dev).manual_seed(seed)
         self.rho_new, self.T_new = [], []  # verified samples collected for fine-tuning
         self.replay = replay  # (rho, T) of the training set, mixed into fine-tuning batches
@@ -217,22 +242,42 @@ class SurrogateSearch:
     def _predict(self, rho: torch.Tensor) -> torch.Tensor:
         return torch.cat([self.net.forward(rho[i:i + 256].float()) for i in range(0, len(rho), 256)])
 
-    def _proposals(self, rho: torch.Tensor) -> torch.Tensor:
-        """n_candidates densities around rho (r, r): steps along the surrogate's gradient
-        of the mean transmission (log-spaced sizes) plus smooth random perturbations."""
-        x = rho[None].float()
-        self.net.forward(x, keep=True)
-        g = self.net.backward(torch.full((1, self.problem.n_freq), 1.0 / self.problem.n_freq, device=self.net.dev),
-                              want_input_grad=True)
+    def _surrogate_grad(self, rho: torch.Tensor) -> torch.Tensor:
+        self.net.forward(rho[None].float(), keep=True)
+        n_out = self.problem.n_freq
+        g = self.net.backward(torch.full((1, n_out), 1.0 / n_out, device=self.net.dev), want_input_grad=True)
         self.net.zero_grad()
-        n = self.n_cand
-        steps = torch.logspace(-2.3, -0.5, n, device=self.net.dev)
-        noise = smooth(torch.randn(n, *rho.shape, generator=self.gen, device=self.net.dev), 3)
-        noise = noise / noise.abs().amax(dim=(1, 2), keepdim=True)
-        amp = torch.rand(n, 1, 1, generator=self.gen, device=self.net.dev) * 0.08
-        gg = g.double().expand(n, -1, -1) / g.abs().max().clamp_min(1e-30)
-        cand = rho[None] + steps.double()[:, None, None] * gg + amp.double() * noise.double()
+        return g[0].double()
+
+    @staticmethod
+    def _unit(d: torch.Tensor) -> torch.Tensor:
+        return d / d.abs().max().clamp_min(1e-30)
+
+    def _steps(self, rho, d, sizes):
+        cand = rho[None] + sizes.double()[:, None, None] * d[None]
         return smooth(cand, 1).clamp(0.0, 1.0)
+
+    def _sizes(self, n):
+        lo, hi = self.ladder
+        return torch.logspace(np.log10(lo), np.log10(hi), n, device=self.net.dev, dtype=torch.float64)
+
+    def _candidates(self, rho, g_adj, g_sur):
+        dirs = [self._unit(g_sur)]
+        if g_adj is not None:
+            ga = self._unit(g_adj)
+            dirs = [ga, dirs[0]] + [self._unit(a * ga + (1 - a) * dirs[0]) for a in (0.25, 0.5, 0.75)]
+        per = 16
+        line = torch.cat([self._steps(rho, d, self._sizes(per)) for d in dirs])
+        n_noise = max(0, self.n_cand - len(line))
+        if n_noise == 0:
+            return line[:self.n_cand]
+        pred = self._predict(line).mean(dim=1)
+        seeds = line[torch.topk(pred, min(8, len(line))).indices]
+        pick = torch.randint(0, len(seeds), (n_noise,), generator=self.gen, device=self.net.dev)
+        noise = smooth(torch.randn(n_noise, *rho.shape, generator=self.gen, device=self.net.dev), 3)
+        noise = noise / noise.abs().amax(dim=(1, 2), keepdim=True)
+        amp = torch.rand(n_noise, 1, 1, generator=self.gen, device=self.net.dev) * 0.06
+        return torch.cat([line, smooth(seeds[pick] + amp.double() * noise.double(), 1).clamp(0.0, 1.0)])
 
     def _finetune(self, steps=10, lr=5e-4):
         if not self.rho_new:
@@ -254,6 +299,10 @@ class SurrogateSearch:
             self.net.backward(2.0 * err / (err.numel() * self.net.y_scale[None, :]))
             self.net.adam_step(lr=lr)
 
+    def _exact_grad(self, rho):
+        _, g = self.problem.value_and_grad(rho[None].cpu().numpy())
+        return torch.as_tensor(g[0], device=self.net.dev)
+
     def run(self, rho0: np.ndarray, rounds: int, target: float | None = None):
         """Optimise from rho0; stops after ``rounds`` or once the verified mean transmission
         reaches ``target``. Returns (best mean T history per round, seconds, best rho)."""
@@ -262,29 +311,39 @@ class SurrogateSearch:
         best = float(self.problem.transmission(rho[None].cpu().numpy()).mean())
         hist = [best]
         t0 = time.perf_counter()
-        pending = None  # exact-adjoint step awaiting verification with the next candidates
+        g_adj = self._exact_grad(rho)  # the first direction is exact
         for rnd in range(rounds):
-            cand = self._proposals(rho)
-            pred = self._predict(cand).mean(dim=1)
-            top = torch.topk(pred, self.n_verify).indices
-            chosen = cand[top]
-            batch = chosen if pending is None else torch.cat([chosen, pending.to(dev)[None]])
+            err, n_rank = 0.0, 0
+            if self.use_surrogate:
+                g_sur = self._surrogate_grad(rho)
+                cand = self._candidates(rho, g_adj, g_sur)
+                pred = self._predict(cand).mean(dim=1)
+                n_rank = self.n_verify - (self.n_anchor if g_adj is not None else 0)
+                ranked = cand[torch.topk(pred, n_rank).indices]
+                pred_ranked = pred[torch.topk(pred, n_rank).indices]
+                parts = [ranked]
+                if g_adj is not None and self.n_anchor:
+                    parts.append(self._steps(rho, self._unit(g_adj),
+                                             self._sizes(self.n_anchor + 2)[1:-1]))
+                batch = torch.cat(parts)
+            else:
+                batch = self._steps(rho, self._unit(g_adj), self._sizes(self.n_verify))
             T_true = self.problem.transmission(batch.cpu().numpy())
             t_true = T_true.mean(axis=1)
-            err = float(np.abs(pred[top].double().cpu().numpy() - t_true[:self.n_verify]).max())
-            self.rho_new.append(chosen.float().cpu().numpy())
-            self.T_new.append(T_true[:self.n_verify].astype(np.float32))
+            if n_rank:
+                err = float(np.abs(pred_ranked.double().cpu().numpy() - t_true[:n_rank]).max())
+                self.rho_new.append(batch[:n_rank].float().cpu().numpy())
+                self.T_new.append(T_true[:n_rank].astype(np.float32))
             k = int(np.argmax(t_true))
-            surrogate_gain = t_true[:self.n_verify].max() > best
-            if t_true[k] > best:
+            improved = t_true[k] > best
+            if improved:
                 best, rho = float(t_true[k]), batch[k]
-            fallback = err > self.tol or not surrogate_gain
-            pending = None
-            if fallback:
-                _, g = self.problem.value_and_grad(rho[None].cpu().numpy())
-                pending = _ascend(rho[None].cpu(), torch.as_tensor(g), self.adjoint_step)[0]
+            fallback = (not self.use_surrogate) or err > self.tol or not improved
+            g_adj = self._exact_grad(rho) if fallback else None
+            if self.use_surrogate and fallback:
                 self._finetune()
-            self.log.append(dict(round=rnd, best=best, surrogate_err=err, fallback=bool(fallback)))
+            self.log.append(dict(round=rnd, best=best, surrogate_err=err, fallback=bool(fallback),
+                                 ranked_best=bool(n_rank and k < n_rank)))
             hist.append(best)
             if target is not None and best >= target:
                 break

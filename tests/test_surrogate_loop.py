@@ -1,0 +1,99 @@
+"""The surrogate search loop on the host with stand-ins for the FDTD problem and the
+network (no GPU): a smooth transmission landscape with its exact gradient, and a
+surrogate that is either exact or corrupted. A corrupted surrogate misses the verified
+transmission by more than the tolerance, so every round falls back to an exact adjoint
+gradient and the loop still climbs on the anchor steps; an exact surrogate is trusted,
+so rounds after an improvement take no adjoint run."""
+import numpy as np
+import torch
+
+from beamz_b200.surrogate.topo import SurrogateSearch
+
+N = 24
+
+
+class FakeProblem:
+    """T(rho) = 1 - mean((rho - target)^2): one 'wavelength', maximum 1 at the target."""
+
+    def __init__(self):
+        g = torch.Generator().manual_seed(3)
+        self.target = torch.rand(N, N, generator=g, dtype=torch.float64) * 0.6 + 0.2
+        self.n_freq = 1
+        self.kw = {"region": (0, 0, N, N)}
+        self.grad_calls = 0
+        self.forward_designs = 0
+
+    def T(self, rho):
+        rho = torch.as_tensor(np.asarray(rho), dtype=torch.float64)
+        return 1.0 - ((rho - self.target) ** 2).mean(dim=(1, 2))
+
+    def transmission(self, rho):
+        self.forward_designs += len(rho)
+        return self.T(rho).numpy()[:, None]
+
+    def value_and_grad(self, rho):
+        self.grad_calls += 1
+        rho_t = torch.as_tensor(np.asarray(rho), dtype=torch.float64)
+        return self.T(rho_t).numpy(), (-2.0 * (rho_t - self.target) / (N * N)).numpy()
+
+
+class FakeNet:
+    """The surrogate interface the loop uses. exact=True predicts the true T (and its
+    gradient); exact=False returns a corrupted constant far from any T."""
+
+    def __init__(self, problem, exact):
+        self.p, self.exact = problem, exact
+        self.dev = torch.device("cpu")
+        self.y_scale = torch.ones(1)
+        self._x = None
+
+    def forward(self, rho, keep=False):
+        self._x = rho.double()
+        if self.exact:
+            return self.p.T(rho.double()).float()[:, None]
+        return torch.full((len(rho), 1), 7.0)
+
+    def backward(self, d_out, want_input_grad=False):
+        x = self._x
+        g = -2.0 * (x - self.p.target) / (N * N) if self.exact else torch.randn(x.shape, dtype=torch.float64)
+        return (g * d_out.double()[:, :1, None]).float() if want_input_grad else None
+
+    def zero_grad(self):
+        pass
+
+    def adam_step(self, lr=1e-3, **kw):
+        pass
+
+
+def _start():
+    return np.full((N, N), 0.5)
+
+
+def test_corrupted_surrogate_falls_back_every_round():
+    prob = FakeProblem()
+    search = SurrogateSearch(prob, FakeNet(prob, exact=False), n_candidates=96, n_verify=8, tol=1e-2)
+    t0 = float(prob.T(_start()[None])[0])
+    hist, _, best = search.run(_start(), rounds=5)
+    assert all(r["fallback"] for r in search.log)
+    assert all(r["surrogate_err"] > 1e-2 for r in search.log)
+    assert prob.grad_calls == 1 + 5  # the first direction plus one exact gradient per round
+    assert hist[-1] > t0 and all(b >= a for a, b in zip(hist, hist[1:]))
+
+
+def test_exact_surrogate_is_trusted():
+    prob = FakeProblem()
+    search = SurrogateSearch(prob, FakeNet(prob, exact=True), n_candidates=96, n_verify=8, tol=1e-2)
+    hist, _, best = search.run(_start(), rounds=4)
+    assert all(r["surrogate_err"] < 1e-6 for r in search.log)
+    trusted = [r for r in search.log if not r["fallback"]]
+    assert trusted, search.log
+    assert prob.grad_calls == 1 + sum(r["fallback"] for r in search.log)
+    assert hist[-1] > hist[0]
+
+
+def test_without_surrogate_is_a_batched_line_search():
+    prob = FakeProblem()
+    search = SurrogateSearch(prob, FakeNet(prob, exact=True), n_candidates=96, n_verify=8, use_surrogate=False)
+    hist, _, _ = search.run(_start(), rounds=3)
+    assert prob.grad_calls == 1 + 3 and prob.forward_designs == 1 + 3 * 8
+    assert hist[-1] > hist[0]
