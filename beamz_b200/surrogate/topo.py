@@ -69,6 +69,7 @@ class TransmissionProblem:
         self.weights = np.ones(self.n_freq)
         self._probs: dict[int, AdjointFDTD2D] = {}
         self.fdtd_designs = 0  # designs simulated (forward runs; an adjoint step counts one)
+        self.fdtd_runs = 0  # solver invocations (one batched forward, or one forward + adjoint)
         self.fdtd_seconds = 0.0
         ref = self._problem(1)
         ref.forward(self.eps(kw["rho_straight"][None]), keep_checkpoints=False)
@@ -98,6 +99,7 @@ class TransmissionProblem:
             p = self._problem(len(chunk))
             p.forward(self.eps(chunk), keep_checkpoints=False)
             out[i:i + len(chunk)] = p.power / self.ref_power[None, :]
+            self.fdtd_runs += 1
         torch.cuda.synchronize()
         self.fdtd_seconds += time.perf_counter() - t0
         self.fdtd_designs += len(rho)
@@ -113,6 +115,7 @@ class TransmissionProblem:
         torch.cuda.synchronize()
         self.fdtd_seconds += time.perf_counter() - t0
         self.fdtd_designs += len(rho)
+        self.fdtd_runs += 1
         g = g * (self.eps_hi - self.eps_lo)
         if return_T:
             return J, g, p.power / self.ref_power[None, :]
@@ -213,11 +216,11 @@ class SurrogateSearch:
          (the exact gradient, the surrogate's gradient and mixes of the two, each scaled
          to a unit peak), and smooth random perturbations of the best-predicted ones;
          each is box-blurred (radius 1) and clipped to [0, 1] as a plain ascent step is;
-      2. verification: ``n_anchor`` steps along the exact gradient at fixed sizes (when
-         it is known) plus the ``n_verify - n_anchor`` candidates the surrogate ranks
-         highest, in one batched FDTD forward; with ``use_surrogate=False`` the whole
-         batch is evenly spaced ladder steps along the exact gradient (the method
-         without the network);
+      2. verification: the ``n_verify`` candidates the surrogate ranks highest plus
+         ``n_anchor`` steps along the exact gradient at fixed sizes (when it is known),
+         in one batched FDTD forward; with ``use_surrogate=False`` the batch is
+         ``n_verify + n_anchor`` evenly spaced ladder steps along the exact gradient (the
+         method without the network);
       3. the best verified design replaces rho when it raises the verified T;
       4. fallback: when the surrogate misses a verified T by more than ``tol`` (or no
          candidate improved), the next round's direction is the exact adjoint gradient
@@ -227,12 +230,12 @@ class SurrogateSearch:
     fell back."""
 
     def __init__(self, problem: TransmissionProblem, net: FNO2d, n_candidates=256, n_verify=16, tol=1e-2,
-                 adjoint_step=0.05, seed=0, replay=None, use_surrogate=True, n_anchor=4, ladder=(0.01, 0.8)):
+                 adjoint_step=0.05, seed=0, replay=None, use_surrogate=True, n_anchor=8, ladder=(0.01, 0.8)):
         self.problem, self.net = problem, net
         self.n_cand, self.n_verify, self.tol = n_candidates, n_verify, tol
         self.adjoint_step = adjoint_step
         self.use_surrogate = use_surrogate
-        self.n_anchor = min(n_anchor, n_verify // 2)
+        self.n_anchor = max(0, int(n_anchor))
         self.ladder = ladder
         self.gen = torch.Generator(device=net.dev).manual_seed(seed)
         self.rho_new, self.T_new = [], []  # verified samples collected for fine-tuning
@@ -318,16 +321,16 @@ class SurrogateSearch:
                 g_sur = self._surrogate_grad(rho)
                 cand = self._candidates(rho, g_adj, g_sur)
                 pred = self._predict(cand).mean(dim=1)
-                n_rank = self.n_verify - (self.n_anchor if g_adj is not None else 0)
-                ranked = cand[torch.topk(pred, n_rank).indices]
-                pred_ranked = pred[torch.topk(pred, n_rank).indices]
+                n_rank = min(self.n_verify, len(cand))
+                top = torch.topk(pred, n_rank).indices
+                ranked, pred_ranked = cand[top], pred[top]
                 parts = [ranked]
                 if g_adj is not None and self.n_anchor:
                     parts.append(self._steps(rho, self._unit(g_adj),
                                              self._sizes(self.n_anchor + 2)[1:-1]))
                 batch = torch.cat(parts)
             else:
-                batch = self._steps(rho, self._unit(g_adj), self._sizes(self.n_verify))
+                batch = self._steps(rho, self._unit(g_adj), self._sizes(self.n_verify + self.n_anchor))
             T_true = self.problem.transmission(batch.cpu().numpy())
             t_true = T_true.mean(axis=1)
             if n_rank:

@@ -71,7 +71,7 @@ def _start():
 
 def test_corrupted_surrogate_falls_back_every_round():
     prob = FakeProblem()
-    search = SurrogateSearch(prob, FakeNet(prob, exact=False), n_candidates=96, n_verify=8, tol=1e-2)
+    search = SurrogateSearch(prob, FakeNet(prob, exact=False), n_candidates=96, n_verify=8, n_anchor=4, tol=1e-2)
     t0 = float(prob.T(_start()[None])[0])
     hist, _, best = search.run(_start(), rounds=5)
     assert all(r["fallback"] for r in search.log)
@@ -82,7 +82,7 @@ def test_corrupted_surrogate_falls_back_every_round():
 
 def test_exact_surrogate_is_trusted():
     prob = FakeProblem()
-    search = SurrogateSearch(prob, FakeNet(prob, exact=True), n_candidates=96, n_verify=8, tol=1e-2)
+    search = SurrogateSearch(prob, FakeNet(prob, exact=True), n_candidates=96, n_verify=8, n_anchor=4, tol=1e-2)
     hist, _, best = search.run(_start(), rounds=4)
     assert all(r["surrogate_err"] < 1e-6 for r in search.log)
     trusted = [r for r in search.log if not r["fallback"]]
@@ -93,7 +93,8 @@ def test_exact_surrogate_is_trusted():
 
 def test_without_surrogate_is_a_batched_line_search():
     prob = FakeProblem()
-    search = SurrogateSearch(prob, FakeNet(prob, exact=True), n_candidates=96, n_verify=8, use_surrogate=False)
+    search = SurrogateSearch(prob, FakeNet(prob, exact=True), n_candidates=96, n_verify=8, n_anchor=4,
+                             use_surrogate=False)
     hist, _, _ = search.run(_start(), rounds=3)
-    assert prob.grad_calls == 1 + 3 and prob.forward_designs == 1 + 3 * 8
+    assert prob.grad_calls == 1 + 3 and prob.forward_designs == 1 + 3 * 12
     assert hist[-1] > hist[0]
