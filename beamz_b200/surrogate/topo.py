@@ -212,22 +212,26 @@ class SurrogateSearch:
 
     Round r, from the current design rho and its exact adjoint gradient g (when the last
     round fell back) or the surrogate's own input gradient (when it did not):
-      1. candidates: steps of a geometric ladder of sizes along the ascent directions
-         (the exact gradient, the surrogate's gradient and mixes of the two, each scaled
-         to a unit peak), and smooth random perturbations of the best-predicted ones;
-         each is box-blurred (radius 1) and clipped to [0, 1] as a plain ascent step is;
+      1. candidates: points along ascent paths followed on the surrogate itself (many
+         small steps of its input gradient, ``_trajectories``), steps of a geometric
+         ladder of sizes along the ascent directions (the exact gradient, the
+         surrogate's gradient and mixes of the two, each scaled to a unit peak), and
+         smooth random perturbations of the best-predicted ones; each is box-blurred
+         (radius 1) and clipped to [0, 1] as a plain ascent step is;
       2. verification: the ``n_verify`` candidates the surrogate ranks highest plus
          ``n_anchor`` steps along the exact gradient at fixed sizes (when it is known),
          in one batched FDTD forward; with ``use_surrogate=False`` the batch is
          ``n_verify + n_anchor`` evenly spaced ladder steps along the exact gradient (the
          method without the network);
       3. the best verified design replaces rho when it raises the verified T;
-      4. fallback: when the surrogate misses a verified T by more than ``tol`` (or no
-         candidate improved), the next round's direction is the exact adjoint gradient
-         at rho (a plain per-design adjoint run); otherwise it is the surrogate's own;
+      4. fallback: when the accepted step's transmission change predicted by the
+         surrogate, dT = T_pred(new) - T_pred(rho), misses the verified change by more
+         than ``tol`` -- or the step was not the network's, or nothing improved -- the
+         next round's direction is the exact adjoint gradient at rho (a plain per-design
+         adjoint run); otherwise it is the surrogate's own;
       5. the verified samples fine-tune the surrogate (mixed with training samples).
-    ``log`` keeps, per round, the best T, the surrogate's largest miss and whether it
-    fell back."""
+    ``log`` keeps, per round, the best T, the error of the accepted step's predicted dT,
+    the surrogate's largest miss of a verified T and whether the round fell back."""
 
     def __init__(self, problem: TransmissionProblem, net: FNO2d, n_candidates=256, n_verify=16, tol=1e-2,
                  adjoint_step=0.05, seed=0, replay=None, use_surrogate=True, n_anchor=8, ladder=(0.01, 0.8)):
@@ -264,13 +268,38 @@ class SurrogateSearch:
         lo, hi = self.ladder
         return torch.logspace(np.log10(lo), np.log10(hi), n, device=self.net.dev, dtype=torch.float64)
 
+    def _trajectories(self, rho, g_adj, n_traj=8, n_inner=24, keep=(1, 2, 4, 6, 9, 13, 18, 24)):
+        """Ascent paths on the surrogate itself: n_traj copies of rho, each stepped n_inner
+        times along the unit-peak input gradient of the surrogate's mean transmission
+        (step sizes spread geometrically over the copies; the first step follows the
+        exact gradient when it is known), blurred and clipped like a plain step; the
+        designs after the steps in ``keep`` are candidates. The network is thus used to
+        follow a curved path that one gradient step cannot."""
+        dev = self.net.dev
+        n_out = self.problem.n_freq
+        sizes = torch.logspace(np.log10(0.02), np.log10(0.12), n_traj, device=dev, dtype=torch.float64)[:, None, None]
+        x = rho[None].expand(n_traj, -1, -1).clone()
+        out = []
+        for i in range(1, n_inner + 1):
+            if i == 1 and g_adj is not None:
+                d = self._unit(g_adj)[None].expand(n_traj, -1, -1)
+            else:
+                self.net.forward(x.float(), keep=True)
+                g = self.net.backward(torch.full((n_traj, n_out), 1.0 / n_out, device=dev), want_input_grad=True)
+                self.net.zero_grad()
+                d = g.double() / g.double().abs().amax(dim=(1, 2), keepdim=True).clamp_min(1e-30)
+            x = smooth(x + sizes * d, 1).clamp(0.0, 1.0)
+            if i in keep:
+                out.append(x.clone())
+        return torch.cat(out)
+
     def _candidates(self, rho, g_adj, g_sur):
         dirs = [self._unit(g_sur)]
         if g_adj is not None:
             ga = self._unit(g_adj)
             dirs = [ga, dirs[0]] + [self._unit(a * ga + (1 - a) * dirs[0]) for a in (0.25, 0.5, 0.75)]
         per = 16
-        line = torch.cat([self._steps(rho, d, self._sizes(per)) for d in dirs])
+        line = torch.cat([self._trajectories(rho, g_adj)] + [self._steps(rho, d, self._sizes(per)) for d in dirs])
         n_noise = max(0, self.n_cand - len(line))
         if n_noise == 0:
             return line[:self.n_cand]
@@ -282,7 +311,7 @@ class SurrogateSearch:
         amp = torch.rand(n_noise, 1, 1, generator=self.gen, device=self.net.dev) * 0.06
         return torch.cat([line, smooth(seeds[pick] + amp.double() * noise.double(), 1).clamp(0.0, 1.0)])
 
-    def _finetune(self, steps=10, lr=5e-4):
+    def _finetune(self, steps=5, lr=5e-4):
         if not self.rho_new:
             return
         dev = self.net.dev
@@ -316,8 +345,9 @@ class SurrogateSearch:
         t0 = time.perf_counter()
         g_adj = self._exact_grad(rho)  # the first direction is exact
         for rnd in range(rounds):
-            err, n_rank = 0.0, 0
+            err, miss, n_rank = float("inf"), 0.0, 0
             if self.use_surrogate:
+                pred_cur = float(self._predict(rho[None]).mean())
                 g_sur = self._surrogate_grad(rho)
                 cand = self._candidates(rho, g_adj, g_sur)
                 pred = self._predict(cand).mean(dim=1)
@@ -333,20 +363,24 @@ class SurrogateSearch:
                 batch = self._steps(rho, self._unit(g_adj), self._sizes(self.n_verify + self.n_anchor))
             T_true = self.problem.transmission(batch.cpu().numpy())
             t_true = T_true.mean(axis=1)
-            if n_rank:
-                err = float(np.abs(pred_ranked.double().cpu().numpy() - t_true[:n_rank]).max())
-                self.rho_new.append(batch[:n_rank].float().cpu().numpy())
-                self.T_new.append(T_true[:n_rank].astype(np.float32))
             k = int(np.argmax(t_true))
             improved = t_true[k] > best
+            if n_rank:
+                pr = pred_ranked.double().cpu().numpy()
+                miss = float(np.abs(pr - t_true[:n_rank]).max())
+                if improved and k < n_rank:  # the accepted step came from the network:
+                    # |dT predicted - dT verified| of that step
+                    err = abs((pr[k] - pred_cur) - (t_true[k] - best))
+                self.rho_new.append(batch[:n_rank].float().cpu().numpy())
+                self.T_new.append(T_true[:n_rank].astype(np.float32))
             if improved:
                 best, rho = float(t_true[k]), batch[k]
-            fallback = (not self.use_surrogate) or err > self.tol or not improved
+            fallback = (not self.use_surrogate) or not improved or err > self.tol
             g_adj = self._exact_grad(rho) if fallback else None
             if self.use_surrogate and fallback:
                 self._finetune()
-            self.log.append(dict(round=rnd, best=best, surrogate_err=err, fallback=bool(fallback),
-                                 ranked_best=bool(n_rank and k < n_rank)))
+            self.log.append(dict(round=rnd, best=best, step_err=(err if np.isfinite(err) else None),
+                                 surrogate_err=miss, fallback=bool(fallback), ranked_best=bool(n_rank and k < n_rank)))
             hist.append(best)
             if target is not None and best >= target:
                 break

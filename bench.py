@@ -714,8 +714,8 @@ def run_surrogate(args):
     same start design, a plain per-design exact-adjoint ascent runs `iterations` steps,
     then the surrogate search (256 candidates per round ranked by the network, the top 16
     verified together with 8 fixed steps along the exact gradient in one batched FDTD
-    forward, exact-adjoint fallback when the network misses a verified T by more than
-    1e-2) and the same search without the network (24 verified designs evenly spaced
+    forward, exact-adjoint fallback when the network's predicted transmission change of
+    the accepted step misses the verified change by more than 1e-2) and the same search without the network (24 verified designs evenly spaced
     along the exact gradient) run until they reach the
     plain ascent's final transmission within 1e-3. designs/s = FDTD-simulated designs
     per second of each loop (an adjoint run counts one design)."""
@@ -778,6 +778,7 @@ def run_surrogate(args):
                           "fallback_rounds": int(sum(r["fallback"] for r in s_["log"])),
                           "rounds_won_by_ranked_candidates": int(sum(r["ranked_best"] for r in s_["log"])),
                           "max_verify_err": round(max(r["surrogate_err"] for r in s_["log"]), 4),
+                          "trusted_rounds": int(sum(not r["fallback"] for r in s_["log"])),
                           "heldout_mae_T": round(mae_v, 4)},
             "without_network": {"final_T": round(n_["hist"][-1], 5), "rounds": len(n_["hist"]) - 1,
                                 "seconds": round(n_["sec"], 3), "fdtd_designs": n_["designs"],

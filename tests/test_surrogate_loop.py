@@ -39,19 +39,20 @@ class FakeProblem:
 
 class FakeNet:
     """The surrogate interface the loop uses. exact=True predicts the true T (and its
-    gradient); exact=False returns a corrupted constant far from any T."""
+    gradient); exact=False returns corrupted predictions: uniform noise in [0, 5)."""
 
     def __init__(self, problem, exact):
         self.p, self.exact = problem, exact
         self.dev = torch.device("cpu")
         self.y_scale = torch.ones(1)
         self._x = None
+        self.gen = torch.Generator().manual_seed(11)
 
     def forward(self, rho, keep=False):
         self._x = rho.double()
         if self.exact:
             return self.p.T(rho.double()).float()[:, None]
-        return torch.full((len(rho), 1), 7.0)
+        return torch.rand((len(rho), 1), generator=self.gen) * 5.0
 
     def backward(self, d_out, want_input_grad=False):
         x = self._x
@@ -76,6 +77,7 @@ def test_corrupted_surrogate_falls_back_every_round():
     hist, _, best = search.run(_start(), rounds=5)
     assert all(r["fallback"] for r in search.log)
     assert all(r["surrogate_err"] > 1e-2 for r in search.log)
+    assert all(r["step_err"] is None or r["step_err"] > 1e-2 for r in search.log)
     assert prob.grad_calls == 1 + 5  # the first direction plus one exact gradient per round
     assert hist[-1] > t0 and all(b >= a for a, b in zip(hist, hist[1:]))
 
@@ -85,6 +87,7 @@ def test_exact_surrogate_is_trusted():
     search = SurrogateSearch(prob, FakeNet(prob, exact=True), n_candidates=96, n_verify=8, n_anchor=4, tol=1e-2)
     hist, _, best = search.run(_start(), rounds=4)
     assert all(r["surrogate_err"] < 1e-6 for r in search.log)
+    assert all(r["step_err"] is None or r["step_err"] < 1e-6 for r in search.log)
     trusted = [r for r in search.log if not r["fallback"]]
     assert trusted, search.log
     assert prob.grad_calls == 1 + sum(r["fallback"] for r in search.log)
