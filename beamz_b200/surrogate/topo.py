@@ -234,7 +234,7 @@ class SurrogateSearch:
     the surrogate's largest miss of a verified T and whether the round fell back."""
 
     def __init__(self, problem: TransmissionProblem, net: FNO2d, n_candidates=256, n_verify=16, tol=1e-2,
-                 adjoint_step=0.05, seed=0, replay=None, use_surrogate=True, n_anchor=8, ladder=(0.01, 0.8)):
+                 adjoint_step=0.05, seed=0, replay=None, use_surrogate=True, n_anchor=16, ladder=(0.01, 0.8)):
         self.problem, self.net = problem, net
         self.n_cand, self.n_verify, self.tol = n_candidates, n_verify, tol
         self.adjoint_step = adjoint_step

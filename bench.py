@@ -713,9 +713,9 @@ def run_surrogate(args):
     (smoothed random ones plus a fraction from batched exact-adjoint ascents); from the
     same start design, a plain per-design exact-adjoint ascent runs `iterations` steps,
     then the surrogate search (256 candidates per round ranked by the network, the top 16
-    verified together with 8 fixed steps along the exact gradient in one batched FDTD
+    verified together with 16 fixed steps along the exact gradient in one batched FDTD
     forward, exact-adjoint fallback when the network's predicted transmission change of
-    the accepted step misses the verified change by more than 1e-2) and the same search without the network (24 verified designs evenly spaced
+    the accepted step misses the verified change by more than 1e-2) and the same search without the network (32 verified designs evenly spaced
     along the exact gradient) run until they reach the
     plain ascent's final transmission within 1e-3. designs/s = FDTD-simulated designs
     per second of each loop (an adjoint run counts one design)."""
@@ -766,7 +766,7 @@ def run_surrogate(args):
             "config": {"workload": "600x400 grid, 120x120 density region, pulsed source, mean mode transmission at "
                                    "1.50-1.60 um (5 wavelengths), 8000 steps; FNO 4 layers x 32 channels x 16 modes",
                        "samples": args.samples, "trajectory_fraction": args.traj_frac, "epochs": args.epochs,
-                       "proposals_per_round": 256, "verified_per_round": "16 ranked + 8 exact-gradient steps",
+                       "proposals_per_round": 256, "verified_per_round": "16 ranked + 16 exact-gradient steps",
                        "fallback_tol": 1e-2,
                        "time_steps": n_steps},
             "plain_per_design": {"value": round(designs_p / sec_p, 3), "unit": "designs/s",

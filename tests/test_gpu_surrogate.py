@@ -207,9 +207,9 @@ def test_fno_with_tcgen05_spectral_gemms_matches_oracle(bz):
 
 
 def test_surrogate_search_beats_plain_adjoint_to_the_same_transmission(bz):
-    """A reduced surrogate run (3000-step problem, 1536 FDTD-labelled samples of which a
-    quarter come from batched exact-adjoint ascents, 12 epochs): from the same start,
-    the surrogate search reaches the final mean transmission of a 10-iteration plain
+    """A reduced surrogate run (the 8000-step problem, 2048 FDTD-labelled samples of
+    which a quarter come from batched exact-adjoint ascents, 12 epochs): from the same start,
+    the surrogate search reaches the final mean transmission of a 15-iteration plain
     per-design adjoint ascent within 1e-3, with fewer solver runs and less wall time;
     the same search without the network (exact-gradient steps only) is reported beside
     it. The plain run also clocks the solver's warm-up, so it goes second."""
@@ -217,14 +217,14 @@ def test_surrogate_search_beats_plain_adjoint_to_the_same_transmission(bz):
     from beamz_b200.surrogate.topo import SurrogateSearch, TransmissionProblem, densities, make_dataset
     from beamz_b200.surrogate.topo import plain_adjoint, train
 
-    prob = TransmissionProblem(n_steps=3000)
-    rho, T = make_dataset(prob, 1536, trajectory_frac=0.25)
+    prob = TransmissionProblem(n_steps=8000)
+    rho, T = make_dataset(prob, 2048, trajectory_frac=0.25)
     net = FNO2d()
     train(net, rho, T, epochs=12)
     rho0 = densities([1234])[0]
     plain_adjoint(prob, rho0, 2)  # warm both problem sizes up
     r0 = prob.fdtd_runs
-    hist_p, sec_p, _ = plain_adjoint(prob, rho0, 10)
+    hist_p, sec_p, _ = plain_adjoint(prob, rho0, 15)
     runs_p = prob.fdtd_runs - r0
     target = hist_p[-1] - 1e-3
     res = {}
