@@ -234,7 +234,7 @@ class SurrogateSearch:
     the surrogate's largest miss of a verified T and whether the round fell back."""
 
     def __init__(self, problem: TransmissionProblem, net: FNO2d, n_candidates=256, n_verify=16, tol=1e-2,
-                 adjoint_step=0.05, seed=0, replay=None, use_surrogate=True, n_anchor=16, ladder=(0.01, 0.8)):
+                 adjoint_step=0.05, seed=0, replay=None, use_surrogate=True, n_anchor=8, ladder=(0.01, 0.8)):
         self.problem, self.net = problem, net
         self.n_cand, self.n_verify, self.tol = n_candidates, n_verify, tol
         self.adjoint_step = adjoint_step
@@ -268,7 +268,7 @@ class SurrogateSearch:
         lo, hi = self.ladder
         return torch.logspace(np.log10(lo), np.log10(hi), n, device=self.net.dev, dtype=torch.float64)
 
-    def _trajectories(self, rho, g_adj, n_traj=8, n_inner=24, keep=(1, 2, 4, 6, 9, 13, 18, 24)):
+    def _trajectories(self, rho, g_adj, n_traj=8, n_inner=16, keep=(1, 2, 3, 5, 8, 12, 16)):
         """Ascent paths on the surrogate itself: n_traj copies of rho, each stepped n_inner
         times along the unit-peak input gradient of the surrogate's mean transmission
         (step sizes spread geometrically over the copies; the first step follows the
@@ -311,7 +311,7 @@ class SurrogateSearch:
         amp = torch.rand(n_noise, 1, 1, generator=self.gen, device=self.net.dev) * 0.06
         return torch.cat([line, smooth(seeds[pick] + amp.double() * noise.double(), 1).clamp(0.0, 1.0)])
 
-    def _finetune(self, steps=5, lr=5e-4):
+    def _finetune(self, steps=3, lr=5e-4):
         if not self.rho_new:
             return
         dev = self.net.dev
@@ -331,19 +331,19 @@ class SurrogateSearch:
             self.net.backward(2.0 * err / (err.numel() * self.net.y_scale[None, :]))
             self.net.adam_step(lr=lr)
 
-    def _exact_grad(self, rho):
-        _, g = self.problem.value_and_grad(rho[None].cpu().numpy())
-        return torch.as_tensor(g[0], device=self.net.dev)
+    def _exact_grad(self, rho, with_value=False):
+        J, g = self.problem.value_and_grad(rho[None].cpu().numpy())
+        g = torch.as_tensor(g[0], device=self.net.dev)
+        return (float(J[0]), g) if with_value else g
 
     def run(self, rho0: np.ndarray, rounds: int, target: float | None = None):
         """Optimise from rho0; stops after ``rounds`` or once the verified mean transmission
         reaches ``target``. Returns (best mean T history per round, seconds, best rho)."""
         dev = self.net.dev
         rho = torch.as_tensor(rho0, dtype=torch.float64, device=dev)
-        best = float(self.problem.transmission(rho[None].cpu().numpy()).mean())
-        hist = [best]
         t0 = time.perf_counter()
-        g_adj = self._exact_grad(rho)  # the first direction is exact
+        best, g_adj = self._exact_grad(rho, with_value=True)  # the first direction is exact
+        hist = [best]
         for rnd in range(rounds):
             err, miss, n_rank = float("inf"), 0.0, 0
             if self.use_surrogate:
