@@ -210,8 +210,9 @@ class SurrogateSearch:
     """Surrogate-ranked ascent of the mean transmission, every accepted design judged by
     a batched FDTD forward run.
 
-    Round r, from the current design rho and its exact adjoint gradient g (when the last
-    round fell back) or the surrogate's own input gradient (when it did not):
+    Round r, from the current design rho, its exact adjoint gradient g (one per-design
+    adjoint run per round: the batched FDTD judges the candidates, the adjoint steers
+    them) and the surrogate's own input gradient:
       1. candidates: points along ascent paths followed on the surrogate itself (many
          small steps of its input gradient, ``_trajectories``), steps of a geometric
          ladder of sizes along the ascent directions (the exact gradient, the
@@ -227,9 +228,11 @@ class SurrogateSearch:
       4. fallback: when the accepted step's transmission change predicted by the
          surrogate, dT = T_pred(new) - T_pred(rho), misses the verified change by more
          than ``tol`` -- or the step was not the network's, or nothing improved -- the
-         next round's direction is the exact adjoint gradient at rho (a plain per-design
-         adjoint run); otherwise it is the surrogate's own;
-      5. the verified samples fine-tune the surrogate (mixed with training samples).
+         round counts as a fallback: its progress came from (or rests on) the exact
+         adjoint steps, and the surrogate is fine-tuned on the verified samples (mixed
+         with training samples) before it proposes again. Steps the network proposes
+         on its own gradient were measured to climb slower than with the exact gradient
+         beside them, so the adjoint run is taken every round.
     ``log`` keeps, per round, the best T, the error of the accepted step's predicted dT,
     the surrogate's largest miss of a verified T and whether the round fell back."""
 
@@ -376,7 +379,7 @@ class SurrogateSearch:
             if improved:
                 best, rho = float(t_true[k]), batch[k]
             fallback = (not self.use_surrogate) or not improved or err > self.tol
-            g_adj = self._exact_grad(rho) if fallback else None
+            g_adj = self._exact_grad(rho)
             if self.use_surrogate and fallback:
                 self._finetune()
             self.log.append(dict(round=rnd, best=best, step_err=(err if np.isfinite(err) else None),

@@ -1,9 +1,8 @@
 """The surrogate search loop on the host with stand-ins for the FDTD problem and the
 network (no GPU): a smooth transmission landscape with its exact gradient, and a
 surrogate that is either exact or corrupted. A corrupted surrogate misses the verified
-transmission by more than the tolerance, so every round falls back to an exact adjoint
-gradient and the loop still climbs on the anchor steps; an exact surrogate is trusted,
-so rounds after an improvement take no adjoint run."""
+transmission change by more than the tolerance, so every round falls back (and the loop
+still climbs on the exact-gradient steps); an exact surrogate is trusted."""
 import numpy as np
 import torch
 
@@ -90,7 +89,7 @@ def test_exact_surrogate_is_trusted():
     assert all(r["step_err"] is None or r["step_err"] < 1e-6 for r in search.log)
     trusted = [r for r in search.log if not r["fallback"]]
     assert trusted, search.log
-    assert prob.grad_calls == 1 + sum(r["fallback"] for r in search.log)
+    assert prob.grad_calls == 1 + len(search.log)
     assert hist[-1] > hist[0]
 
 
