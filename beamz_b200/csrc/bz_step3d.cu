@@ -630,9 +630,13 @@ __device__ __forceinline__ void quad_segment(const Ptr3<float>& in, const Out3<f
   }
 }
 
-// One block per (x tile, y tile, z block of ZB planes, design-component).
+// One block per (x tile, y tile, z block of ZB planes, design-component). Blocks per SM
+// the register budget is sized for (8-row tiles): BZ_QUAD_MIN_BLOCKS.
+#ifndef BZ_QUAD_MIN_BLOCKS
+#define BZ_QUAD_MIN_BLOCKS 2
+#endif
 template <int ZB, int TY>
-__global__ void __launch_bounds__(TX * TY, TY == 8 ? 2 : 1) step3d_quad_kernel(Ptr3<float> in, Out3<float> out,
+__global__ void __launch_bounds__(TX * TY, TY == 8 ? BZ_QUAD_MIN_BLOCKS : 1) step3d_quad_kernel(Ptr3<float> in, Out3<float> out,
                                                                   const float* __restrict__ ce,
                                                                   const float* __restrict__ loss,
                                                                   Geo3D<float> g) {

@@ -1,11 +1,13 @@
 #!/usr/bin/env python
-"""Benchmark of the FDTD stepping path: Gcell-updates/s on the 2D MMI workload.
+"""Benchmark of the FDTD stepping path: Gcell-updates/s.
 
-Workload (default ``mmi_2d``): 2000 x 1000 cells at 20 nm, Si 1x2 MMI in SiO2,
-30-cell order-3 PML, CW mode source, DFT flux monitors at 5 wavelengths on the
-input and both output ports, 20000 time steps. One bench step = one full run of
-all 20000 time steps from zero fields. The grid (fields + coefficients, 64 MB)
-fits in L2, so L2 is flushed (a 512 MB write) before every run.
+Workload (default ``soi_mmi_3d``): the 3D SOI strip + 6 x 3 um MMI, 600 x 300 x 150
+cells at 20 nm, 16-cell PML on all faces, Gaussian-pulse mode source, 5-wavelength DFT
+flux planes on both outputs, 8000 time steps. One bench step = one full run of all time
+steps from zero fields; fields and coefficients (1.5 GB) exceed L2. ``--workload
+mmi_2d | dipole_2d`` select the 2D configurations (their grids fit in L2, which is then
+flushed with a 512 MB write before every run), ``topo_2d`` the batched adjoint and
+``surrogate_2d`` the surrogate search.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
 
@@ -13,10 +15,8 @@ Prints one JSON line (rank 0). With N > 1 (torchrun) every rank runs its own
 replica of the workload ("replicas only": the path has no exchange step); value
 is the total cell updates of all ranks over the slowest rank's time.
 
-``--impl reference`` times the reference algorithm's CPU implementation (the
-float64 NumPy restatement in oracle/, operation-for-operation the reference's
-NumPy backend and step helpers) on a bounded sample of the same workload, one
-independent copy per host core (at most 64), reporting their aggregate rate.
+``--impl reference`` times the reference package itself (installed under
+baseline/_ref) on the host cores, on the same workload and config: see run_reference.
 """
 from __future__ import annotations
 

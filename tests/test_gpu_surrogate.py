@@ -207,7 +207,7 @@ def test_fno_with_tcgen05_spectral_gemms_matches_oracle(bz):
 
 
 def test_surrogate_search_beats_plain_adjoint_to_the_same_transmission(bz):
-    """A reduced surrogate run (the 8000-step problem, 4096 FDTD-labelled samples of
+    """A reduced surrogate run (the 8000-step problem, 8192 FDTD-labelled samples of
     which half come from batched exact-adjoint ascents, 15 epochs): from the same start,
     the surrogate search reaches the final mean transmission of a 15-iteration plain
     per-design adjoint ascent within 1e-3, with fewer solver runs and less wall time;
@@ -218,7 +218,7 @@ def test_surrogate_search_beats_plain_adjoint_to_the_same_transmission(bz):
     from beamz_b200.surrogate.topo import plain_adjoint, train
 
     prob = TransmissionProblem(n_steps=8000)
-    rho, T = make_dataset(prob, 4096, trajectory_frac=0.5)
+    rho, T = make_dataset(prob, 8192, trajectory_frac=0.5)
     net = FNO2d()
     train(net, rho, T, epochs=15)
     rho0 = densities([1234])[0]
