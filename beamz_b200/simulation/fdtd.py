@@ -228,15 +228,19 @@ class FDTD:
 
     def _run_until_end(self):
         """Steps to the end, in graph chunks between the steps that need host copies."""
-        while self.current_step < self.num_steps:
-            n_free = self._next_save(self.current_step) - self.current_step
+        self._run_until(self.num_steps)
+
+    def _run_until(self, stop: int):
+        stop = min(int(stop), self.num_steps)
+        while self.current_step < stop:
+            n_free = min(self._next_save(self.current_step), stop) - self.current_step
             if n_free > 0:
                 self.engine.run_steps(n_free)
                 # t advances by repeated addition, as one step at a time would
                 # (accumulate adds in order, so the rounding is the same)
                 self.t = float(np.add.accumulate(np.r_[self.t, np.full(n_free, self.dt)])[-1])
                 self.current_step += n_free
-            if self.current_step < self.num_steps:
+            if self.current_step < stop:
                 self.step()
 
     def _collect_monitors(self):
@@ -323,6 +327,48 @@ class FDTD:
         self.initialize_simulation(save=save, live=live, axis_scale=axis_scale, save_fields=save_fields,
                                    decimate_save=decimate_save, accumulate_power=accumulate_power,
                                    save_memory_mode=save_memory_mode, fields_to_cache=fields_to_cache)
+        self._run_until_end()
+        return self.finalize_simulation()
+
+    # ---- partial runs and checkpoints (no counterpart in the reference) -------------
+    def run_for(self, n_steps: int, **run_kwargs) -> None:
+        """Advance n_steps (initialising first, with run()'s keyword arguments, if the
+        simulation has not started); finalise with finalize_simulation() or continue."""
+        if self.engine is None:
+            self.initialize_simulation(**run_kwargs)
+        self._run_until(self.current_step + int(n_steps))
+
+    def save_checkpoint(self, path) -> None:
+        """Write the run's state after the steps taken so far: fields (both copies),
+        monitor DFT sums and records, accumulated power, step index, time and saved
+        results (``simulation.checkpoint``). Resuming after a whole number of graph
+        chunks continues with the bits of the uninterrupted run."""
+        import torch
+
+        from .checkpoint import engine_state
+
+        if self.engine is None:
+            raise RuntimeError("nothing to save: the simulation has not started")
+        st = engine_state(self.engine)
+        st["fdtd"] = {"current_step": self.current_step, "t": self.t, "t_host": getattr(self, "_t_host", 0.0),
+                      "results": {k: list(v) for k, v in self.results.items()}}
+        torch.save(st, path)
+
+    def resume(self, path, **run_kwargs) -> Dict:
+        """Continue a run from a save_checkpoint file: initialise with run()'s keyword
+        arguments, restore the state, step to the end and finalise (returns results)."""
+        import torch
+
+        from .checkpoint import load_engine_state
+
+        self.initialize_simulation(**run_kwargs)
+        st = torch.load(path, weights_only=False)
+        load_engine_state(self.engine, st)
+        f = st["fdtd"]
+        self.current_step, self.t = int(f["current_step"]), f["t"]
+        self._t_host = f.get("t_host", 0.0)
+        for k, v in f["results"].items():
+            self.results[k] = list(v)
         self._run_until_end()
         return self.finalize_simulation()
 
