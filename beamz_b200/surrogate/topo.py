@@ -271,7 +271,7 @@ class SurrogateSearch:
         lo, hi = self.ladder
         return torch.logspace(np.log10(lo), np.log10(hi), n, device=self.net.dev, dtype=torch.float64)
 
-    def _trajectories(self, rho, g_adj, n_traj=16, n_inner=12, keep=(1, 2, 3, 4, 6, 8, 10, 12)):
+    def _trajectories(self, rho, g_adj, n_traj=8, n_inner=24, keep=(1, 2, 4, 6, 9, 13, 18, 24)):
         """Ascent paths on the surrogate itself: n_traj copies of rho, each stepped n_inner
         times along the unit-peak input gradient of the surrogate's mean transmission
         (step sizes spread geometrically over the copies; the first step follows the
@@ -280,7 +280,7 @@ class SurrogateSearch:
         follow a curved path that one gradient step cannot."""
         dev = self.net.dev
         n_out = self.problem.n_freq
-        sizes = torch.logspace(np.log10(0.02), np.log10(0.16), n_traj, device=dev, dtype=torch.float64)[:, None, None]
+        sizes = torch.logspace(np.log10(0.02), np.log10(0.12), n_traj, device=dev, dtype=torch.float64)[:, None, None]
         x = rho[None].expand(n_traj, -1, -1).clone()
         out = []
         for i in range(1, n_inner + 1):
@@ -314,7 +314,7 @@ class SurrogateSearch:
         amp = torch.rand(n_noise, 1, 1, generator=self.gen, device=self.net.dev) * 0.06
         return torch.cat([line, smooth(seeds[pick] + amp.double() * noise.double(), 1).clamp(0.0, 1.0)])
 
-    def _finetune(self, steps=2, lr=5e-4):
+    def _finetune(self, steps=3, lr=5e-4):
         if not self.rho_new:
             return
         dev = self.net.dev
