@@ -486,16 +486,13 @@ struct QuadIn {
   float ez_x, ey_x;  // E at x+4 (the warp's last lane)
 };
 
-// One column segment: tile (bx, by) of design/component dc, planes [z0, z1). NB = 2:
-// the shared tiles are double-buffered by plane parity and the E tile of plane k+1 (the
-// old E, already in registers) is stored before the one barrier of plane k, so each
-// plane needs one block barrier instead of two. NB = 1: two barriers per plane.
-template <int TY, int NB>
+// One column segment: tile (bx, by) of design/component dc, planes [z0, z1).
+template <int TY>
 __device__ __forceinline__ void quad_segment(const Ptr3<float>& in, const Out3<float>& out,
                                              const float* __restrict__ ce, const float* __restrict__ loss,
                                              const Geo3D<float>& g, int bx, int by, int dc, int z0, int z1,
-                                             float4 (*s_ez)[TY][TX], float4 (*s_ex)[TY][TX],
-                                             float4 (*s_hz)[TY][TX], float4 (*s_hx)[TY][TX]) {
+                                             float4 (*s_ez)[TX], float4 (*s_ex)[TX], float4 (*s_hz)[TX],
+                                             float4 (*s_hx)[TX]) {
   const int tx = threadIdx.x, ty = threadIdx.y;
   const int nx = g.nx, ny = g.ny, nz = g.nz;
   const int x = bx * (4 * TX - 4) - 4 + 4 * tx;  // first cell of the quad
@@ -556,14 +553,8 @@ __device__ __forceinline__ void quad_segment(const Ptr3<float>& in, const Out3<f
     }
   }
 
-  if (NB == 2) {  // E tile of the first plane
-    s_ez[z0 & 1][ty][tx] = ezk;
-    s_ex[z0 & 1][ty][tx] = exk;
-    __syncthreads();
-  }
   for (int k = z0; k < z1; ++k) {
     const long long po = (long long)k * P + col;
-    const int b = NB == 2 ? (k & 1) : 0;
     float4 ex2, ey2, ez2;  // prefetch: inputs of plane k+1 and E(k+2)
     if (k + 1 < z1) {
       load_plane(k + 1, nxt);
@@ -572,13 +563,11 @@ __device__ __forceinline__ void quad_segment(const Ptr3<float>& in, const Out3<f
       ey2 = ld4(in.e[1], o, inb && k + 2 < nz);
       ez2 = ld4(in.e[2], o, inb && k + 2 < nz);
     }
-    if (NB == 1) {
-      s_ez[0][ty][tx] = ezk;
-      s_ex[0][ty][tx] = exk;
-      __syncthreads();
-    }
-    const float4 ez_yp = ye ? cur.ez_y : s_ez[b][ty + (ye ? 0 : 1)][tx];
-    const float4 ex_yp = ye ? cur.ex_y : s_ex[b][ty + (ye ? 0 : 1)][tx];
+    s_ez[ty][tx] = ezk;
+    s_ex[ty][tx] = exk;
+    __syncthreads();
+    const float4 ez_yp = ye ? cur.ez_y : s_ez[ty + (ye ? 0 : 1)][tx];
+    const float4 ex_yp = ye ? cur.ex_y : s_ex[ty + (ye ? 0 : 1)][tx];
     float ez_x4 = __shfl_down_sync(FULL, ezk.x, 1);
     float ey_x4 = __shfl_down_sync(FULL, eyk.x, 1);
     if (xe) {
@@ -598,19 +587,15 @@ __device__ __forceinline__ void quad_segment(const Ptr3<float>& in, const Out3<f
       q_at(hzn, j) = fh * q_get(cur.hz, j) - (cx * (ey_xp - eyc) - cy * (q_get(ex_yp, j) - exc));
       q_at(fe4, j) = 1.f - q_get(cur.a, j) * q_get(cur.ce, j) * g.inv_kd2;
     }
-    s_hz[b][ty][tx] = hzn;
-    s_hx[b][ty][tx] = hxn;
-    if (NB == 2 && k + 1 < z1) {  // the old E of plane k+1, for H(k+1) after this barrier
-      s_ez[b ^ 1][ty][tx] = ezn;
-      s_ex[b ^ 1][ty][tx] = exn;
-    }
+    s_hz[ty][tx] = hzn;
+    s_hx[ty][tx] = hxn;
     __syncthreads();
     const float hy_xm = __shfl_up_sync(FULL, hyn.w, 1);
     const float hz_xm = __shfl_up_sync(FULL, hzn.w, 1);
     if (owned) {
       const long long o = fb + po;
-      const float4 hz_ym = s_hz[b][ty - 1][tx];
-      const float4 hx_ym = s_hx[b][ty - 1][tx];
+      const float4 hz_ym = s_hz[ty - 1][tx];
+      const float4 hx_ym = s_hx[ty - 1][tx];
       const bool kin = k >= 1 && k <= nz - 2, kz = k <= nz - 2;
       float4 ex = exk, ey = eyk, ez = ezk;
 #pragma unroll
@@ -645,26 +630,16 @@ __device__ __forceinline__ void quad_segment(const Ptr3<float>& in, const Out3<f
   }
 }
 
-// One block per (x tile, y tile, z block of ZB planes, design-component). Blocks per SM
-// the register budget is sized for (8-row tiles): BZ_QUAD_MIN_BLOCKS.
-#ifndef BZ_QUAD_MIN_BLOCKS
-#define BZ_QUAD_MIN_BLOCKS 2
-#endif
-// Shared-tile buffers of 8-row tiles: 2 (one barrier per plane) or 1 (two barriers).
-#ifndef BZ_QUAD_BUFFERS
-#define BZ_QUAD_BUFFERS 2
-#endif
+// One block per (x tile, y tile, z block of ZB planes, design-component).
 template <int ZB, int TY>
-__global__ void __launch_bounds__(TX * TY, TY == 8 ? BZ_QUAD_MIN_BLOCKS : 1) step3d_quad_kernel(Ptr3<float> in, Out3<float> out,
+__global__ void __launch_bounds__(TX * TY, TY == 8 ? 2 : 1) step3d_quad_kernel(Ptr3<float> in, Out3<float> out,
                                                                   const float* __restrict__ ce,
                                                                   const float* __restrict__ loss,
                                                                   Geo3D<float> g) {
-  constexpr int NB = TY == 8 ? BZ_QUAD_BUFFERS : 1;  // 16-row tiles: one buffer (48 KB static limit)
-  __shared__ float4 s_ez[NB][TY][TX], s_ex[NB][TY][TX], s_hz[NB][TY][TX], s_hx[NB][TY][TX];
+  __shared__ float4 s_ez[TY][TX], s_ex[TY][TX], s_hz[TY][TX], s_hx[TY][TX];
   const int dc = blockIdx.z / g.nzb;
   const int z0 = (blockIdx.z - dc * g.nzb) * ZB;
-  quad_segment<TY, NB>(in, out, ce, loss, g, blockIdx.x, blockIdx.y, dc, z0, min(z0 + ZB, g.nz), s_ez, s_ex, s_hz,
-                       s_hx);
+  quad_segment<TY>(in, out, ce, loss, g, blockIdx.x, blockIdx.y, dc, z0, min(z0 + ZB, g.nz), s_ez, s_ex, s_hz, s_hx);
 }
 
 template <int TY>
