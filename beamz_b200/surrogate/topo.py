@@ -379,12 +379,12 @@ class SurrogateSearch:
             if improved:
                 best, rho = float(t_true[k]), batch[k]
             fallback = (not self.use_surrogate) or not improved or err > self.tol
-            g_adj = self._exact_grad(rho)
-            if self.use_surrogate and fallback:
-                self._finetune()
             self.log.append(dict(round=rnd, best=best, step_err=(err if np.isfinite(err) else None),
                                  surrogate_err=miss, fallback=bool(fallback), ranked_best=bool(n_rank and k < n_rank)))
             hist.append(best)
             if target is not None and best >= target:
-                break
+                break  # done: no gradient is needed at the final design (plain ascent takes none either)
+            g_adj = self._exact_grad(rho)
+            if self.use_surrogate and fallback:
+                self._finetune()
         return hist, time.perf_counter() - t0, rho.cpu().numpy()
