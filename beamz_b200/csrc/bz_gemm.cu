@@ -10,7 +10,10 @@
 // of bank conflicts), double buffered, and multiplied by warps with
 // mma.sync.m16n8k16 (bf16 inputs, f32 accumulators). The epilogue adds an f32
 // term, row/column biases, applies GELU, and stores f32 and/or bf16, or
-// accumulates atomically (batch-reduced or split-K weight gradients).
+// accumulates atomically (batch-reduced or split-K weight gradients). Where the
+// shapes allow, bz_gemm_bf16 runs tcgen05/TMEM kernels instead: the large DFT GEMMs
+// (TMA-fed, 128 x 256 tiles) and the 1x1 channel mixing (pixel-contiguous
+// activations as an MN-major TMA operand); both are described below.
 #include <cuda.h>
 #include <cuda_bf16.h>
 
@@ -701,6 +704,230 @@ bool tc_eligible(const GemmP& p) {
          p.sa % 8 == 0 && p.sb % 8 == 0 && al(p.A) && al(p.B);
 }
 
+// ---- tcgen05 channel mixing: C[b] = epilogue(W (M x K) @ X[b] (K x N)), X pixel-contiguous ----
+// The surrogate's 1x1 layers: X[b] is [K][N] with the N pixels contiguous and W a small
+// weight (M, K in {32, 64}) shared by the batch. Computed transposed, D[b] (N x M) =
+// X[b]^T W^T: the pixels are the MMA's M (128 per tile), the output channels its N.
+// X is therefore an MN-major A operand. TMA stages it with 128-byte swizzling as two
+// 64-pixel boxes of K rows per tile; that is the MN-major SWIZZLE_128B layout of the
+// descriptor (8-row atoms of 128-byte rows along K, atoms SBO = 1024 bytes apart, the
+// second 64-pixel block LBO = 128 K bytes after the first; a K step of 16 moves the
+// start address by two atoms). W^T is the K-major B operand, written once per CTA by
+// the threads in the no-swizzle core-matrix layout. A CTA of 128 threads walks tiles
+// (design b, 128 pixels) with a MIX_S-stage TMA ring: per tile, thread 0 issues K/16
+// MMAs into M TMEM columns and commits them; the four warps read their 32 pixels' rows
+// with tcgen05.ld and apply the epilogue (f32 term, biases, pre-activation, GELU), every
+// load and store coalesced along the pixels. Memory-bound (K = 32: 64 bytes read and
+// 64-192 bytes written per pixel), so several CTAs share an SM and their epilogues
+// keep loads in flight. Bounded waits as in the GEMMs above.
+namespace mix {
+constexpr int S = 4, TP = 128, THREADS = 128;
+}
+
+// MN-major SWIZZLE_128B operand descriptor: LBO = distance between the 64-element MN
+// blocks, SBO = 1024 bytes between 8-row K atoms, sm_100 version bits, layout type 2.
+__device__ __forceinline__ uint64_t tc_sdesc_sw128_mn(uint32_t saddr, uint32_t lbo) {
+  uint64_t d = (uint64_t)((saddr >> 4) & 0x3FFFu);
+  d |= (uint64_t)((lbo >> 4) & 0x3FFFu) << 16;
+  d |= (uint64_t)(1024 >> 4) << 32;
+  d |= (uint64_t)1 << 46;
+  d |= (uint64_t)2 << 61;
+  return d;
+}
+
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&v)[32]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+      "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];\n"
+      : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]), "=r"(v[8]),
+        "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15]), "=r"(v[16]),
+        "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]), "=r"(v[22]), "=r"(v[23]), "=r"(v[24]),
+        "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+}
+
+template <int KC, int MC>
+struct MixCfg {
+  static constexpr int A_ST = 2 * KC * 128;  // two 64-pixel boxes of KC rows (bytes)
+  static constexpr int W_OFF = mix::S * A_ST;
+  static constexpr int LBO_W = (MC / 8) * 128;
+  static constexpr int BAR_OFF = W_OFF + MC * KC * 2;
+  static constexpr int SMEM = BAR_OFF + 8 * (mix::S + 2) + 1024;  // + alignment slack
+  static constexpr int NCOL = MC < 32 ? 32 : MC;
+  static constexpr uint32_t IDESC = (1u << 4) | (1u << 7) | (1u << 10) | (1u << 15) | ((uint32_t)(MC >> 3) << 17) |
+                                    ((uint32_t)(mix::TP >> 4) << 24);  // f32 += bf16 x bf16, A MN-major
+};
+
+template <int KC, int MC>
+__global__ void __launch_bounds__(mix::THREADS) mix_tc_kernel(const __grid_constant__ CUtensorMap tmX, GemmP p,
+                                                             int n_tiles, int tiles_n) {
+  using C = MixCfg<KC, MC>;
+  extern __shared__ unsigned char smem_raw[];
+  unsigned char* smem = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  unsigned char* bar = smem + C::BAR_OFF;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bar + 8 * (mix::S + 1));
+  const uint32_t sbase = static_cast<uint32_t>(__cvta_generic_to_shared(smem));
+  const uint32_t full0 = static_cast<uint32_t>(__cvta_generic_to_shared(bar)), mdone = full0 + 8 * mix::S;
+
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(
+                     static_cast<uint32_t>(__cvta_generic_to_shared(tmem_slot))),
+                 "r"(C::NCOL));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::);
+  }
+  if (tid == 0) {
+    for (int i = 0; i <= mix::S; ++i) asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(full0 + 8 * i));
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  }
+  // W^T (rows = output channels m, K contiguous) in the no-swizzle K-major layout
+  for (int i = tid; i < MC * KC; i += mix::THREADS) {
+    const int m = i / KC, k = i - (i / KC) * KC;
+    const bf16 w = p.ta ? p.A[(long long)k * p.lda + m] : p.A[(long long)m * p.lda + k];
+    *reinterpret_cast<bf16*>(smem + C::W_OFF + (k >> 3) * C::LBO_W + (m >> 3) * 128 + (m & 7) * 16 + (k & 7) * 2) = w;
+  }
+  asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+  asm volatile("tcgen05.fence::before_thread_sync;\n" ::);
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
+  const uint32_t taddr = *tmem_slot;
+
+  const int n_my = (n_tiles - (int)blockIdx.x + (int)gridDim.x - 1) / (int)gridDim.x;
+  auto issue = [&](int j) {  // this CTA's tile j into stage j % S
+    const int t = (int)blockIdx.x + j * (int)gridDim.x;
+    const int b = t / tiles_n, n0 = (t - b * tiles_n) * mix::TP;
+    const uint32_t st = sbase + (j % mix::S) * C::A_ST, fb = full0 + 8 * (j % mix::S);
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(fb), "r"(C::A_ST) : "memory");
+    tma_load_2d(st, &tmX, n0, b * KC, fb);
+    tma_load_2d(st + KC * 128, &tmX, n0 + 64, b * KC, fb);
+  };
+  int ok = 1, issued = 0, consumed = 0;
+  if (tid == 0)
+    for (; issued < min(mix::S, n_my); ++issued) issue(issued);
+  for (int j = 0; j < n_my; ++j) {
+    const int t = (int)blockIdx.x + j * (int)gridDim.x;
+    const int b = t / tiles_n, n0 = (t - b * tiles_n) * mix::TP;
+    const int s = j % mix::S;
+    if (tid == 0) {
+      if (!tc_wait(full0 + 8 * s, (uint32_t)((j / mix::S) & 1), p.wait_limit)) {
+        ok = 0;
+      } else {
+        consumed = j + 1;
+        asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
+        const uint32_t a0 = sbase + s * C::A_ST, b0 = sbase + C::W_OFF;
+#pragma unroll
+        for (int kk = 0; kk < KC / 16; ++kk) {
+          const uint64_t da = tc_sdesc_sw128_mn(a0 + kk * 2048, KC * 128);
+          const uint64_t db = tc_sdesc(b0 + kk * 2 * C::LBO_W, C::LBO_W, 128);
+          asm volatile(
+              "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+              "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n"
+              :
+              : "r"(taddr), "l"(da), "l"(db), "r"(C::IDESC), "r"(kk > 0 ? 1u : 0u), "r"(0u), "r"(0u), "r"(0u),
+                "r"(0u));
+        }
+        asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(mdone));
+      }
+    }
+    if (!__syncthreads_and(ok)) {
+      ok = 0;
+      break;
+    }
+    ok = tc_wait(mdone, (uint32_t)(j & 1), p.wait_limit) ? 1 : 0;  // this tile's MMAs
+    if (!__syncthreads_and(ok)) {
+      ok = 0;
+      break;
+    }
+    asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
+    if (tid == 0 && issued < n_my) issue(issued++);  // stage s is free again
+    const int n = n0 + warp * 32 + lane;
+    const bool live = n < p.N;
+#pragma unroll
+    for (int c0 = 0; c0 < MC; c0 += 32) {
+      uint32_t v[32];
+      tmem_ld32(taddr + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, v);
+      if (!live) continue;
+      float x[32];
+#pragma unroll
+      for (int e = 0; e < 32; ++e) x[e] = p.alpha * __uint_as_float(v[e]);
+      if (p.cadd) {
+        const float* q = p.cadd + (long long)b * p.sadd + (long long)c0 * p.ldadd + n;
+#pragma unroll
+        for (int e = 0; e < 32; ++e) x[e] += __ldg(q + (long long)e * p.ldadd);
+      }
+#pragma unroll
+      for (int e = 0; e < 32; ++e) {
+        const int m = c0 + e;
+        float y = x[e];
+        if (p.bias_m) y += __ldg(p.bias_m + m);
+        if (p.bias_n) y += __ldg(p.bias_n + n);
+        if (p.pre) p.pre[(long long)b * p.spre + (long long)m * p.ldpre + n] = __float2bfloat16_rn(y);
+        if (p.act == 1) y = gelu_f(y);
+        const long long o = (long long)b * p.sc + (long long)m * p.ldc + n;
+        if (p.outf) p.outf[o] = y;
+        if (p.outh) p.outh[o] = __float2bfloat16_rn(y);
+      }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;\n" ::);
+    __syncthreads();  // TMEM read out before the next tile's MMAs overwrite it
+  }
+  if (tid == 0) {
+    if (!ok && consumed > 0) tc_wait(mdone, (uint32_t)((consumed - 1) & 1), p.wait_limit);  // let issued MMAs drain
+    for (int t = consumed; t < issued; ++t)  // copies still in flight after a failure
+      tc_wait(full0 + 8 * (t % mix::S), (uint32_t)((t / mix::S) & 1), p.wait_limit);
+    if (!ok) atomicExch(&g_tc_error, 1);
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;\n" ::);
+  __syncthreads();
+  if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(taddr), "r"(C::NCOL));
+}
+
+// The mixing kernel takes: one weight for the whole batch (sa == 0), X (B operand,
+// tb == 0) pixel-contiguous with the designs back to back (sb == K * ldb), K and M in
+// {32, 64}, a plain or fused epilogue without atomics or split-K, 16-byte aligned rows.
+bool mix_eligible(const GemmP& p) {
+  auto al = [](const void* q) { return (reinterpret_cast<uintptr_t>(q) & 15u) == 0u; };
+  return !p.tb && !p.atomic && p.splitk == 1 && p.sa == 0 && (p.K == 32 || p.K == 64) && (p.M == 32 || p.M == 64) &&
+         p.N >= 64 && p.ldb % 8 == 0 && p.sb == (long long)p.K * p.ldb && al(p.B) &&
+         (long long)p.batch * p.K <= (1LL << 31) - 1;
+}
+
+template <int KC, int MC>
+int launch_mix_kc_mc(const GemmP& p, cudaStream_t st) {
+  using C = MixCfg<KC, MC>;
+  static int per_sm = 0;
+  if (per_sm == 0) {
+    if (cudaFuncSetAttribute(mix_tc_kernel<KC, MC>, cudaFuncAttributeMaxDynamicSharedMemorySize, C::SMEM) !=
+        cudaSuccess)
+      return fail(BZ_ERR_CUDA, "bz_gemm_bf16: cannot configure the mixing kernel's shared memory");
+    int n = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, mix_tc_kernel<KC, MC>, mix::THREADS, C::SMEM) !=
+            cudaSuccess ||
+        n < 1)
+      return fail(BZ_ERR_CUDA, "bz_gemm_bf16: the mixing kernel does not fit on an SM");
+    per_sm = min(n, 512 / C::NCOL);  // TMEM columns of the resident CTAs
+  }
+  alignas(64) CUtensorMap mx;
+  if (!make_map(&mx, p.B, (long long)p.batch * KC, p.N, p.ldb, KC)) return 0;
+  int dev = 0, sms = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const int tiles_n = (int)ceil_div(p.N, mix::TP);
+  const long long n_tiles = (long long)p.batch * tiles_n;
+  if (n_tiles > (1LL << 31) - 1) return 0;
+  const int grid = (int)(n_tiles < (long long)sms * per_sm ? n_tiles : (long long)sms * per_sm);
+  mix_tc_kernel<KC, MC><<<grid, mix::THREADS, C::SMEM, st>>>(mx, p, (int)n_tiles, tiles_n);
+  const int rc = check_launch("bz_gemm_bf16");
+  return rc == BZ_OK ? 1 : rc;
+}
+
+// 1: launched; 0: not applicable (caller uses another kernel); <0: error status.
+int launch_mix(const GemmP& p, cudaStream_t st) {
+  if (p.K == 32) return p.M == 32 ? launch_mix_kc_mc<32, 32>(p, st) : launch_mix_kc_mc<32, 64>(p, st);
+  return p.M == 32 ? launch_mix_kc_mc<64, 32>(p, st) : launch_mix_kc_mc<64, 64>(p, st);
+}
+
 // ---- spectral channel mixing: O[b][o][k] = sum_c U[b][c][k] * W[k][c][o] (complex) ---
 // U, O: [B][C][n_modes][2] bf16 (re, im); W: [n_modes][Ci][Co][2] bf16. One block per
 // mode: the mode's weights and a chunk of SB designs' coefficients are staged in shared
@@ -906,6 +1133,10 @@ extern "C" int bz_gemm_bf16(const bz_gemm* g, void* stream) {
     const int t = bz::launch_gemm_tma(p, st);
     if (t != 0) return t > 0 ? BZ_OK : t;
     return bz::launch_gemm_tc(p, st);
+  }
+  if (g->engine == 0 && bz::mix_eligible(p)) {
+    const int t = bz::launch_mix(p, st);
+    if (t != 0) return t > 0 ? BZ_OK : t;
   }
   if (g->engine == 2 && bz::tc_eligible(p)) return bz::launch_gemm_tc(p, st);
   if (g->N <= 32) return bz::launch_gemm<128, 32, 4, 1>(p, st);

@@ -388,3 +388,20 @@ class SurrogateSearch:
             if self.use_surrogate and fallback:
                 self._finetune()
         return hist, time.perf_counter() - t0, rho.cpu().numpy()
+
+
+def active_learning(problem: TransmissionProblem, net: FNO2d, starts: np.ndarray, rounds: int = 4, replay=None,
+                    **search_kw) -> dict:
+    """Fine-tunes a trained surrogate on its own proposals: a search of ``rounds`` rounds
+    from each start design (no target), whose FDTD-verified candidates fine-tune the
+    network on every fallback round as in ``SurrogateSearch.run``. Part of training: the
+    start designs must not include the one a timed search starts from. Returns the
+    seconds, FDTD-simulated designs and the best T reached from each start."""
+    t0 = time.perf_counter()
+    d0 = problem.fdtd_designs
+    best = []
+    for i, rho0 in enumerate(np.asarray(starts)):
+        s = SurrogateSearch(problem, net, replay=replay, seed=1000 + i, **search_kw)
+        hist, _, _ = s.run(rho0, rounds=rounds)
+        best.append(hist[-1])
+    return {"seconds": time.perf_counter() - t0, "fdtd_designs": problem.fdtd_designs - d0, "best_T": best}

@@ -418,9 +418,12 @@ int bz_rasterize3d(int32_t nx, int32_t ny, int32_t nz, int32_t n_zs, const doubl
 typedef struct bz_gemm {
   int32_t M, N, K, batch, splitk, act;
   int32_t ta, tb, atomic;
-  int32_t engine;               /* 0: tcgen05/TMEM kernels where eligible (ta = 0, tb = 1,
-                                   M >= 128, N >= 256, K >= 64, 16-byte aligned rows; TMA-fed
-                                   when batch = 1), else mma.sync; 1: mma.sync only;
+  int32_t engine;               /* 0: tcgen05/TMEM kernels where eligible, else mma.sync:
+                                   the GEMM kernel for ta = 0, tb = 1, M >= 128, N >= 256,
+                                   K >= 64, 16-byte aligned rows (TMA-fed when batch = 1); the
+                                   channel-mixing kernel for tb = 0, K and M in {32, 64},
+                                   N >= 64, sb = K * ldb, no atomic / split-K;
+                                   1: mma.sync only;
                                    2: the register-staged tcgen05 kernel where eligible */
   const void* A;
   int64_t lda, sa;

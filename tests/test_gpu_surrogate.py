@@ -182,6 +182,55 @@ def test_tcgen05_gemm_matches_mma_sync_and_f32(bz, M, N, K, batch, split):
         assert rel(outs[engine], outs[1]) <= 1e-5, engine
 
 
+@pytest.mark.parametrize("K,M", [(32, 32), (32, 64), (64, 32), (64, 64)])
+@pytest.mark.parametrize("ta", [0, 1])
+@pytest.mark.parametrize("N", [14400, 200])
+def test_tcgen05_channel_mixing_matches_mma_sync_and_f32(bz, K, M, ta, N):
+    """The tcgen05 channel-mixing kernel (engine 0: a weight shared by the batch times
+    pixel-contiguous activations, X the MN-major operand by TMA) against the mma.sync
+    kernel (engine 1) and an f32 matmul of the same bf16 operands, with every epilogue
+    term (f32 add, both biases, pre-activation copy, GELU, f32 and bf16 outputs);
+    N = 200 leaves a partial 128-pixel tile and a fully out-of-range TMA box."""
+    from beamz_b200 import _native as nat
+
+    g = torch.Generator().manual_seed(K * 1000 + M * 10 + ta + N)
+    batch = 3
+    W = torch.randn(M, K, generator=g).to(torch.bfloat16)
+    X = torch.randn(batch, K, N, generator=g).to(torch.bfloat16)
+    add = torch.randn(batch, M, N, generator=g)
+    bm, bn = torch.randn(M, generator=g), torch.randn(N, generator=g)
+    lin = torch.einsum("mk,bkn->bmn", W.float(), X.float()) * 0.5 + add + bm[None, :, None] + bn[None, None, :]
+    dev = "cuda"
+    Wd = (W.t() if ta else W).contiguous().to(dev)
+    Xd, addd, bmd, bnd = X.to(dev), add.to(dev), bm.to(dev), bn.to(dev)
+    res = {}
+    nat.gemm_error(reset=True)
+    for engine in (0, 1):
+        outf = torch.empty(batch, M, N, device=dev)
+        outh = torch.empty(batch, M, N, device=dev, dtype=torch.bfloat16)
+        pre = torch.empty_like(outh)
+        p = nat.Gemm()
+        p.M, p.N, p.K, p.batch, p.splitk, p.act, p.ta, p.tb, p.atomic = M, N, K, batch, 1, 1, ta, 0, 0
+        p.engine = engine
+        p.A, p.lda, p.sa = Wd.data_ptr(), (M if ta else K), 0
+        p.B, p.ldb, p.sb = Xd.data_ptr(), N, K * N
+        p.alpha = 0.5
+        p.cadd, p.ldadd, p.sadd = addd.data_ptr(), N, M * N
+        p.bias_m, p.bias_n = bmd.data_ptr(), bnd.data_ptr()
+        p.outf, p.outh, p.ldc, p.sc = outf.data_ptr(), outh.data_ptr(), N, M * N
+        p.pre, p.ldpre, p.spre = pre.data_ptr(), N, M * N
+        nat.gemm(p, torch.cuda.current_stream().cuda_stream)
+        torch.cuda.synchronize()
+        res[engine] = (outf, outh, pre)
+    assert nat.gemm_error(reset=True) == 0
+    want = fno_ref.gelu(lin.double())
+    outf, outh, pre = res[0]
+    assert rel(outf, want) <= 1e-5
+    assert rel(outh.float(), want) <= 8e-3
+    assert rel(pre.float(), lin) <= 8e-3
+    assert rel(outf, res[1][0]) <= 1e-5
+
+
 def test_fno_with_tcgen05_spectral_gemms_matches_oracle(bz):
     """n = 64, 8 modes, width 32, batch 8: the DFT GEMMs (M = 256, N = 256, K = 4096)
     and their inverses run on the tcgen05 kernel."""

@@ -6,7 +6,7 @@ still climbs on the exact-gradient steps); an exact surrogate is trusted."""
 import numpy as np
 import torch
 
-from beamz_b200.surrogate.topo import SurrogateSearch
+from beamz_b200.surrogate.topo import SurrogateSearch, active_learning
 
 N = 24
 
@@ -21,6 +21,7 @@ class FakeProblem:
         self.kw = {"region": (0, 0, N, N)}
         self.grad_calls = 0
         self.forward_designs = 0
+        self.fdtd_designs = 0
 
     def T(self, rho):
         rho = torch.as_tensor(np.asarray(rho), dtype=torch.float64)
@@ -28,10 +29,12 @@ class FakeProblem:
 
     def transmission(self, rho):
         self.forward_designs += len(rho)
+        self.fdtd_designs += len(rho)
         return self.T(rho).numpy()[:, None]
 
     def value_and_grad(self, rho):
         self.grad_calls += 1
+        self.fdtd_designs += len(rho)
         rho_t = torch.as_tensor(np.asarray(rho), dtype=torch.float64)
         return self.T(rho_t).numpy(), (-2.0 * (rho_t - self.target) / (N * N)).numpy()
 
@@ -46,6 +49,7 @@ class FakeNet:
         self.y_scale = torch.ones(1)
         self._x = None
         self.gen = torch.Generator().manual_seed(11)
+        self.adam_steps = 0
 
     def forward(self, rho, keep=False):
         self._x = rho.double()
@@ -62,7 +66,7 @@ class FakeNet:
         pass
 
     def adam_step(self, lr=1e-3, **kw):
-        pass
+        self.adam_steps += 1
 
 
 def _start():
@@ -100,3 +104,27 @@ def test_without_surrogate_is_a_batched_line_search():
     hist, _, _ = search.run(_start(), rounds=3)
     assert prob.grad_calls == 1 + 3 and prob.forward_designs == 3 * 12
     assert hist[-1] > hist[0]
+
+
+def test_search_stops_at_the_target_without_a_further_gradient():
+    """Once the verified T reaches the target the loop ends: no exact gradient is taken
+    at the final design (the plain ascent takes none there either)."""
+    prob = FakeProblem()
+    t0 = float(prob.T(_start()[None])[0])
+    search = SurrogateSearch(prob, FakeNet(prob, exact=True), n_candidates=96, n_verify=8, n_anchor=4)
+    hist, _, _ = search.run(_start(), rounds=10, target=t0 + 1e-9)
+    assert len(search.log) == 1 and hist[-1] >= t0 + 1e-9
+    assert prob.grad_calls == 1
+
+
+def test_active_learning_fine_tunes_on_its_own_proposals():
+    """Searches from each start (no target): with a corrupted surrogate every round falls
+    back and fine-tunes the network (3 Adam steps per round); the FDTD count is the
+    verified batches plus one gradient per round and the initial one per start."""
+    prob = FakeProblem()
+    net = FakeNet(prob, exact=False)
+    starts = np.stack([_start(), np.full((N, N), 0.3)])
+    st = active_learning(prob, net, starts, rounds=3, n_candidates=96, n_verify=8, n_anchor=4)
+    assert net.adam_steps == 2 * 3 * 3
+    assert st["fdtd_designs"] == 2 * 3 * (8 + 4) + 2 * (1 + 3)
+    assert len(st["best_T"]) == 2 and st["seconds"] >= 0
