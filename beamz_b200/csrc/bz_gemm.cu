@@ -753,8 +753,8 @@ struct MixCfg {
   static constexpr int W_OFF = mix::S * A_ST;
   static constexpr int LBO_W = (MC / 8) * 128;
   static constexpr int BAR_OFF = W_OFF + MC * KC * 2;
-  static constexpr int SMEM = BAR_OFF + 8 * (mix::S + 2) + 1024;  // + alignment slack
-  static constexpr int NCOL = MC < 32 ? 32 : MC;
+  static constexpr int SMEM = BAR_OFF + 8 * (mix::S + 3) + 1024;  // + alignment slack
+  static constexpr int NCOL = MC < 32 ? 32 : MC;                   // columns of one accumulator
   static constexpr uint32_t IDESC = (1u << 4) | (1u << 7) | (1u << 10) | (1u << 15) | ((uint32_t)(MC >> 3) << 17) |
                                     ((uint32_t)(mix::TP >> 4) << 24);  // f32 += bf16 x bf16, A MN-major
 };
@@ -767,18 +767,19 @@ __global__ void __launch_bounds__(mix::THREADS) mix_tc_kernel(const __grid_const
   unsigned char* smem = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   unsigned char* bar = smem + C::BAR_OFF;
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bar + 8 * (mix::S + 1));
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bar + 8 * (mix::S + 2));
   const uint32_t sbase = static_cast<uint32_t>(__cvta_generic_to_shared(smem));
-  const uint32_t full0 = static_cast<uint32_t>(__cvta_generic_to_shared(bar)), mdone = full0 + 8 * mix::S;
+  // barriers: full[S] (TMA), mdone[2] (MMAs of the accumulator pair)
+  const uint32_t full0 = static_cast<uint32_t>(__cvta_generic_to_shared(bar)), mdone0 = full0 + 8 * mix::S;
 
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(
                      static_cast<uint32_t>(__cvta_generic_to_shared(tmem_slot))),
-                 "r"(C::NCOL));
+                 "r"(2 * C::NCOL));
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::);
   }
   if (tid == 0) {
-    for (int i = 0; i <= mix::S; ++i) asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(full0 + 8 * i));
+    for (int i = 0; i < mix::S + 2; ++i) asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(full0 + 8 * i));
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
   }
   // W^T (rows = output channels m, K contiguous) in the no-swizzle K-major layout
@@ -802,64 +803,65 @@ __global__ void __launch_bounds__(mix::THREADS) mix_tc_kernel(const __grid_const
     tma_load_2d(st, &tmX, n0, b * KC, fb);
     tma_load_2d(st + KC * 128, &tmX, n0 + 64, b * KC, fb);
   };
-  int ok = 1, issued = 0, consumed = 0;
-  if (tid == 0)
+  // tile j's MMAs into accumulator j & 1 (thread 0); false when its operands never landed
+  auto mma = [&](int j) -> bool {
+    const int s = j % mix::S;
+    if (!tc_wait(full0 + 8 * s, (uint32_t)((j / mix::S) & 1), p.wait_limit)) return false;
+    asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
+    const uint32_t a0 = sbase + s * C::A_ST, b0 = sbase + C::W_OFF, d = taddr + (uint32_t)((j & 1) * C::NCOL);
+#pragma unroll
+    for (int kk = 0; kk < KC / 16; ++kk) {
+      const uint64_t da = tc_sdesc_sw128_mn(a0 + kk * 2048, KC * 128);
+      const uint64_t db = tc_sdesc(b0 + kk * 2 * C::LBO_W, C::LBO_W, 128);
+      asm volatile(
+          "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+          "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n"
+          :
+          : "r"(d), "l"(da), "l"(db), "r"(C::IDESC), "r"(kk > 0 ? 1u : 0u), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
+    }
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(
+        mdone0 + 8 * (j & 1)));
+    return true;
+  };
+  int ok = 1, issued = 0, mmas = 0;
+  if (tid == 0) {
     for (; issued < min(mix::S, n_my); ++issued) issue(issued);
-  for (int j = 0; j < n_my; ++j) {
+    if (mma(0)) mmas = 1; else ok = 0;
+  }
+  ok = __syncthreads_and(ok);
+  for (int j = 0; j < n_my && ok; ++j) {
     const int t = (int)blockIdx.x + j * (int)gridDim.x;
     const int b = t / tiles_n, n0 = (t - b * tiles_n) * mix::TP;
-    const int s = j % mix::S;
-    if (tid == 0) {
-      if (!tc_wait(full0 + 8 * s, (uint32_t)((j / mix::S) & 1), p.wait_limit)) {
-        ok = 0;
-      } else {
-        consumed = j + 1;
-        asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
-        const uint32_t a0 = sbase + s * C::A_ST, b0 = sbase + C::W_OFF;
+    const int n = n0 + warp * 32 + lane;
+    const bool live = n < p.N;
+    // the f32 term of this tile: independent of the MMAs, so its loads go first
+    float add[MC];
 #pragma unroll
-        for (int kk = 0; kk < KC / 16; ++kk) {
-          const uint64_t da = tc_sdesc_sw128_mn(a0 + kk * 2048, KC * 128);
-          const uint64_t db = tc_sdesc(b0 + kk * 2 * C::LBO_W, C::LBO_W, 128);
-          asm volatile(
-              "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
-              "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n"
-              :
-              : "r"(taddr), "l"(da), "l"(db), "r"(C::IDESC), "r"(kk > 0 ? 1u : 0u), "r"(0u), "r"(0u), "r"(0u),
-                "r"(0u));
-        }
-        asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(mdone));
-      }
+    for (int e = 0; e < MC; ++e) add[e] = 0.f;
+    if (p.cadd && live) {
+      const float* q = p.cadd + (long long)b * p.sadd + n;
+#pragma unroll
+      for (int e = 0; e < MC; ++e) add[e] = __ldg(q + (long long)e * p.ldadd);
     }
-    if (!__syncthreads_and(ok)) {
-      ok = 0;
-      break;
+    if (tid == 0 && j + 1 < n_my) {  // next tile into the other accumulator (read out by iteration j - 1)
+      if (mma(j + 1)) mmas = j + 2; else ok = 0;
     }
-    ok = tc_wait(mdone, (uint32_t)(j & 1), p.wait_limit) ? 1 : 0;  // this tile's MMAs
+    if (!tc_wait(mdone0 + 8 * (j & 1), (uint32_t)((j >> 1) & 1), p.wait_limit)) ok = 0;
     if (!__syncthreads_and(ok)) {
       ok = 0;
       break;
     }
     asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
-    if (tid == 0 && issued < n_my) issue(issued++);  // stage s is free again
-    const int n = n0 + warp * 32 + lane;
-    const bool live = n < p.N;
+    if (tid == 0 && issued < n_my) issue(issued++);  // tile j's stage is free again
 #pragma unroll
     for (int c0 = 0; c0 < MC; c0 += 32) {
       uint32_t v[32];
-      tmem_ld32(taddr + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, v);
+      tmem_ld32(taddr + ((uint32_t)(warp * 32) << 16) + (uint32_t)((j & 1) * C::NCOL + c0), v);
       if (!live) continue;
-      float x[32];
-#pragma unroll
-      for (int e = 0; e < 32; ++e) x[e] = p.alpha * __uint_as_float(v[e]);
-      if (p.cadd) {
-        const float* q = p.cadd + (long long)b * p.sadd + (long long)c0 * p.ldadd + n;
-#pragma unroll
-        for (int e = 0; e < 32; ++e) x[e] += __ldg(q + (long long)e * p.ldadd);
-      }
 #pragma unroll
       for (int e = 0; e < 32; ++e) {
         const int m = c0 + e;
-        float y = x[e];
+        float y = p.alpha * __uint_as_float(v[e]) + add[m];
         if (p.bias_m) y += __ldg(p.bias_m + m);
         if (p.bias_n) y += __ldg(p.bias_n + n);
         if (p.pre) p.pre[(long long)b * p.spre + (long long)m * p.ldpre + n] = __float2bfloat16_rn(y);
@@ -870,17 +872,19 @@ __global__ void __launch_bounds__(mix::THREADS) mix_tc_kernel(const __grid_const
       }
     }
     asm volatile("tcgen05.fence::before_thread_sync;\n" ::);
-    __syncthreads();  // TMEM read out before the next tile's MMAs overwrite it
+    __syncthreads();  // accumulator j & 1 read out before tile j + 2's MMAs overwrite it
   }
   if (tid == 0) {
-    if (!ok && consumed > 0) tc_wait(mdone, (uint32_t)((consumed - 1) & 1), p.wait_limit);  // let issued MMAs drain
-    for (int t = consumed; t < issued; ++t)  // copies still in flight after a failure
+    if (!ok && mmas > 0)  // let issued MMAs drain before the TMEM goes
+      tc_wait(mdone0 + 8 * ((mmas - 1) & 1), (uint32_t)(((mmas - 1) >> 1) & 1), p.wait_limit);
+    for (int t = mmas; t < issued; ++t)  // copies still in flight after a failure
       tc_wait(full0 + 8 * (t % mix::S), (uint32_t)((t / mix::S) & 1), p.wait_limit);
     if (!ok) atomicExch(&g_tc_error, 1);
   }
   asm volatile("tcgen05.fence::before_thread_sync;\n" ::);
   __syncthreads();
-  if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(taddr), "r"(C::NCOL));
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(taddr), "r"(2 * C::NCOL));
 }
 
 // The mixing kernel takes: one weight for the whole batch (sa == 0), X (B operand,
@@ -899,14 +903,20 @@ int launch_mix_kc_mc(const GemmP& p, cudaStream_t st) {
   static int per_sm = 0;
   if (per_sm == 0) {
     if (cudaFuncSetAttribute(mix_tc_kernel<KC, MC>, cudaFuncAttributeMaxDynamicSharedMemorySize, C::SMEM) !=
-        cudaSuccess)
-      return fail(BZ_ERR_CUDA, "bz_gemm_bf16: cannot configure the mixing kernel's shared memory");
-    int n = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, mix_tc_kernel<KC, MC>, mix::THREADS, C::SMEM) !=
             cudaSuccess ||
-        n < 1)
-      return fail(BZ_ERR_CUDA, "bz_gemm_bf16: the mixing kernel does not fit on an SM");
-    per_sm = min(n, 512 / C::NCOL);  // TMEM columns of the resident CTAs
+        cudaFuncSetAttribute(mix_tc_kernel<KC, MC>, cudaFuncAttributePreferredSharedMemoryCarveout, 100) !=
+            cudaSuccess)
+      return fail(BZ_ERR_CUDA, "bz_gemm_bf16: cannot configure the mixing kernel's shared memory");
+    // resident CTAs per SM from the kernel's registers (allocated per warp in units of
+    // 256), its shared memory (1 KB reserved per CTA) and the 512 TMEM columns
+    cudaFuncAttributes fa;
+    int dev = 0, smem_sm = 0;
+    if (cudaFuncGetAttributes(&fa, mix_tc_kernel<KC, MC>) != cudaSuccess || cudaGetDevice(&dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev) != cudaSuccess)
+      return fail(BZ_ERR_CUDA, "bz_gemm_bf16: cannot query the mixing kernel's resources");
+    const int regs_cta = ((fa.numRegs * 32 + 255) / 256 * 256) * (mix::THREADS / 32);
+    const int by_regs = 65536 / max(1, regs_cta), by_smem = smem_sm / (C::SMEM + 1024);
+    per_sm = max(1, min(min(by_regs, by_smem), min(8, 512 / (2 * C::NCOL))));
   }
   alignas(64) CUtensorMap mx;
   if (!make_map(&mx, p.B, (long long)p.batch * KC, p.N, p.ldb, KC)) return 0;

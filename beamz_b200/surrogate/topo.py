@@ -236,7 +236,7 @@ class SurrogateSearch:
     ``log`` keeps, per round, the best T, the error of the accepted step's predicted dT,
     the surrogate's largest miss of a verified T and whether the round fell back."""
 
-    def __init__(self, problem: TransmissionProblem, net: FNO2d, n_candidates=256, n_verify=16, tol=1e-2,
+    def __init__(self, problem: TransmissionProblem, net: FNO2d, n_candidates=256, n_verify=24, tol=1e-2,
                  adjoint_step=0.05, seed=0, replay=None, use_surrogate=True, n_anchor=8, ladder=(0.01, 0.8)):
         self.problem, self.net = problem, net
         self.n_cand, self.n_verify, self.tol = n_candidates, n_verify, tol

@@ -710,19 +710,22 @@ def run_topo(args):
 def run_surrogate(args):
     """surrogate_2d: the topology problem with a pulsed source and mean transmission over
     1.50-1.60 um. An FNO surrogate (bf16 kernels) is trained on FDTD-labelled densities
-    (smoothed random ones plus a fraction from batched exact-adjoint ascents); from the
-    same start design, a plain per-design exact-adjoint ascent runs `iterations` steps,
-    then the surrogate search (256 candidates per round ranked by the network, the top 16
-    verified together with 8 fixed steps along the exact gradient in one batched FDTD
-    forward, exact-adjoint fallback when the network's predicted transmission change of
-    the accepted step misses the verified change by more than 1e-2) and the same search without the network (24 verified designs evenly spaced
-    along the exact gradient) run until they reach the
-    plain ascent's final transmission within 1e-3. designs/s = FDTD-simulated designs
-    per second of each loop (an adjoint run counts one design)."""
+    (smoothed random ones plus a fraction from batched exact-adjoint ascents), then
+    fine-tuned on its own verified proposals by searches from three other start designs
+    (active learning, reported with the training). From one start design, a plain
+    per-design exact-adjoint ascent runs `iterations` steps, then the surrogate search
+    (256 candidates per round ranked by the network, the top 24 verified together with 8
+    fixed steps along the exact gradient in one batched FDTD forward, exact-adjoint
+    fallback when the network's predicted transmission change of the accepted step
+    misses the verified change by more than 1e-2) and the same search without the
+    network (32 verified designs evenly spaced along the exact gradient) run until they
+    reach the plain ascent's final transmission within 1e-3. designs/s = FDTD-simulated
+    designs per second of each loop (an adjoint run counts one design)."""
     import torch
 
     from beamz_b200.surrogate.fno import FNO2d
-    from beamz_b200.surrogate.topo import SurrogateSearch, TransmissionProblem, densities, make_dataset, plain_adjoint
+    from beamz_b200.surrogate.topo import SurrogateSearch, TransmissionProblem, active_learning, densities
+    from beamz_b200.surrogate.topo import make_dataset, plain_adjoint
     from beamz_b200.surrogate.topo import train as train_fno
 
     torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
@@ -739,6 +742,9 @@ def run_surrogate(args):
     torch.cuda.synchronize()
     t_train = time.perf_counter() - t0
     train_tflops = net.flops / t_train / 1e12
+    # active learning (part of training): searches from three other start designs whose
+    # FDTD-verified proposals fine-tune the network
+    active = active_learning(prob, net, densities([50001, 50002, 50003]), rounds=4, replay=(rho, T))
     rho_v = densities(range(90000, 90256))
     T_v = prob.transmission(rho_v)
     pred_v = torch.cat([net.forward(torch.as_tensor(rho_v[i:i + 64], device=net.dev)) for i in range(0, 256, 64)])
@@ -766,7 +772,8 @@ def run_surrogate(args):
             "config": {"workload": "600x400 grid, 120x120 density region, pulsed source, mean mode transmission at "
                                    "1.50-1.60 um (5 wavelengths), 8000 steps; FNO 4 layers x 32 channels x 16 modes",
                        "samples": args.samples, "trajectory_fraction": args.traj_frac, "epochs": args.epochs,
-                       "proposals_per_round": 256, "verified_per_round": "16 ranked + 8 exact-gradient steps",
+                       "proposals_per_round": 256, "verified_per_round": "24 ranked + 8 exact-gradient steps",
+                       "active_learning": "4 search rounds from each of 3 other start designs before timing",
                        "fallback_tol": 1e-2,
                        "time_steps": n_steps},
             "plain_per_design": {"value": round(designs_p / sec_p, 3), "unit": "designs/s",
@@ -791,7 +798,9 @@ def run_surrogate(args):
             "dataset": {"seconds": round(t_data, 1), "fdtd_gcells_per_s": round(args.samples * cells * n_steps /
                                                                                 t_data / 1e9, 1)},
             "training": {"seconds": round(t_train, 1), "best_epoch": fit["best_epoch"],
-                         "val_mae_T": round(min(fit["val"]), 4), "tensor_tflops": round(train_tflops, 1)},
+                         "val_mae_T": round(min(fit["val"]), 4), "tensor_tflops": round(train_tflops, 1),
+                         "active_learning_seconds": round(active["seconds"], 1),
+                         "active_learning_fdtd_designs": active["fdtd_designs"]},
             "T_stats": {"train_mean": round(float(T.mean()), 4), "train_std": round(float(T.std()), 4),
                         "train_max": round(float(T.max()), 4)},
             "rounds_log": [{k: (round(v, 4) if isinstance(v, float) else v) for k, v in r.items()}
