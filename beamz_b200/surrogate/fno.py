@@ -293,3 +293,54 @@ def bench_step(batch: int = 64, steps: int = 10, warmup: int = 3) -> float:
     b.record()
     torch.cuda.synchronize()
     return a.elapsed_time(b) / max(1, steps)
+
+
+def bench_mixing(reps: int = 20) -> list:
+    """The 1x1 channel-mixing GEMMs of the default FNO at batch 64 (120 x 120 pixels)
+    through bz_gemm_bf16 with engine 0 (the tcgen05 mixing kernel) and engine 1
+    (mma.sync): microseconds per launch (CUDA events over ``reps`` back-to-back launches,
+    operands and outputs of 120-300 MB, above the 126 MB L2) and the algorithmic bytes
+    per second (activations read, f32 term read, pre-activation and output written)."""
+    dev = torch.device("cuda")
+    B, P = 64, 120 * 120
+    st = torch.cuda.current_stream().cuda_stream
+    rows = []
+    # (M, K, ta, fused): the forward layer (f32 term, bias, pre-activation, GELU), the head's
+    # first layer, the head's transposed layer in the backward, a transposed layer with
+    # the f32 term (backward through a Fourier layer)
+    for M, K, ta, fused in ((32, 32, 0, True), (64, 32, 0, True), (32, 64, 1, False), (32, 32, 1, True)):
+        W = torch.randn(M, K, device=dev).to(BF16)
+        Wd = (W.t() if ta else W).contiguous()
+        X = torch.randn(B, K, P, device=dev).to(BF16)
+        add = torch.randn(B, M, P, device=dev) if fused else None
+        bias = torch.randn(M, device=dev)
+        outh = torch.empty(B, M, P, device=dev, dtype=BF16)
+        pre = torch.empty_like(outh) if fused else None
+        row = {"M": M, "K": K, "ta": ta, "fused": fused}
+        for engine in (0, 1):
+            g = nat.Gemm()
+            g.M, g.N, g.K, g.batch, g.splitk, g.act, g.ta, g.tb, g.atomic = M, P, K, B, 1, int(fused), ta, 0, 0
+            g.engine = engine
+            g.A, g.lda, g.sa = Wd.data_ptr(), (M if ta else K), 0
+            g.B, g.ldb, g.sb = X.data_ptr(), P, K * P
+            g.alpha = 1.0
+            if fused:
+                g.cadd, g.ldadd, g.sadd = add.data_ptr(), P, M * P
+                g.bias_m = bias.data_ptr()
+                g.pre, g.ldpre, g.spre = pre.data_ptr(), P, M * P
+            g.outh, g.ldc, g.sc = outh.data_ptr(), P, M * P
+            for _ in range(3):
+                nat.gemm(g, st)
+            torch.cuda.synchronize()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            for _ in range(reps):
+                nat.gemm(g, st)
+            b.record()
+            torch.cuda.synchronize()
+            us = a.elapsed_time(b) / reps * 1e3
+            nbytes = B * P * (2 * K + 2 * M + (6 * M if fused else 0))
+            row["tcgen05_us" if engine == 0 else "mma_sync_us"] = round(us, 1)
+            row["tcgen05_gbs" if engine == 0 else "mma_sync_gbs"] = round(nbytes / us / 1e3)
+        rows.append(row)
+    return rows
