@@ -55,6 +55,15 @@ __device__ __forceinline__ float gelu_f(float v) {
   return 0.5f * v * (1.0f + tanhf(u));
 }
 
+// GELU (tanh form) for results stored only as bf16: the PTX tanh.approx.f32 instruction
+// (relative error about 2^-11) is below the 2^-9 rounding of the bf16 store.
+__device__ __forceinline__ float gelu_bf16out(float v) {
+  const float u = 0.7978845608028654f * (v + 0.044715f * v * v * v);
+  float t;
+  asm("tanh.approx.f32 %0, %1;" : "=f"(t) : "f"(u));
+  return 0.5f * v * (1.0f + t);
+}
+
 __device__ __forceinline__ float gelu_grad(float v) {
   const float u = 0.7978845608028654f * (v + 0.044715f * v * v * v);
   const float t = tanhf(u);
@@ -788,6 +797,8 @@ __global__ void __launch_bounds__(mix::THREADS) mix_tc_kernel(const __grid_const
     const bf16 w = p.ta ? p.A[(long long)k * p.lda + m] : p.A[(long long)m * p.lda + k];
     *reinterpret_cast<bf16*>(smem + C::W_OFF + (k >> 3) * C::LBO_W + (m >> 3) * 128 + (m & 7) * 16 + (k & 7) * 2) = w;
   }
+  __shared__ float s_bias[MC];
+  for (int i = tid; i < MC; i += mix::THREADS) s_bias[i] = p.bias_m ? p.bias_m[i] : 0.f;
   asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
   asm volatile("tcgen05.fence::before_thread_sync;\n" ::);
   __syncthreads();
@@ -853,22 +864,34 @@ __global__ void __launch_bounds__(mix::THREADS) mix_tc_kernel(const __grid_const
     }
     asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
     if (tid == 0 && issued < n_my) issue(issued++);  // tile j's stage is free again
+    const float bn = (p.bias_n && live) ? __ldg(p.bias_n + n) : 0.f;
 #pragma unroll
     for (int c0 = 0; c0 < MC; c0 += 32) {
       uint32_t v[32];
       tmem_ld32(taddr + ((uint32_t)(warp * 32) << 16) + (uint32_t)((j & 1) * C::NCOL + c0), v);
       if (!live) continue;
+      // output rows walked by pointer increments (one 64-bit add per element and array)
+      bf16* pq = p.pre ? p.pre + (long long)b * p.spre + (long long)c0 * p.ldpre + n : nullptr;
+      const long long o0 = (long long)b * p.sc + (long long)c0 * p.ldc + n;
+      float* fq = p.outf ? p.outf + o0 : nullptr;
+      bf16* hq = p.outh ? p.outh + o0 : nullptr;
 #pragma unroll
       for (int e = 0; e < 32; ++e) {
         const int m = c0 + e;
-        float y = p.alpha * __uint_as_float(v[e]) + add[m];
-        if (p.bias_m) y += __ldg(p.bias_m + m);
-        if (p.bias_n) y += __ldg(p.bias_n + n);
-        if (p.pre) p.pre[(long long)b * p.spre + (long long)m * p.ldpre + n] = __float2bfloat16_rn(y);
-        if (p.act == 1) y = gelu_f(y);
-        const long long o = (long long)b * p.sc + (long long)m * p.ldc + n;
-        if (p.outf) p.outf[o] = y;
-        if (p.outh) p.outh[o] = __float2bfloat16_rn(y);
+        float y = p.alpha * __uint_as_float(v[e]) + add[m] + s_bias[m] + bn;
+        if (pq) {
+          *pq = __float2bfloat16_rn(y);
+          pq += p.ldpre;
+        }
+        if (p.act == 1) y = fq ? gelu_f(y) : gelu_bf16out(y);
+        if (fq) {
+          *fq = y;
+          fq += p.ldc;
+        }
+        if (hq) {
+          *hq = __float2bfloat16_rn(y);
+          hq += p.ldc;
+        }
       }
     }
     asm volatile("tcgen05.fence::before_thread_sync;\n" ::);
@@ -915,7 +938,7 @@ int launch_mix_kc_mc(const GemmP& p, cudaStream_t st) {
         cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev) != cudaSuccess)
       return fail(BZ_ERR_CUDA, "bz_gemm_bf16: cannot query the mixing kernel's resources");
     const int regs_cta = ((fa.numRegs * 32 + 255) / 256 * 256) * (mix::THREADS / 32);
-    const int by_regs = 65536 / max(1, regs_cta), by_smem = smem_sm / (C::SMEM + 1024);
+    const int by_regs = 65536 / max(1, regs_cta), by_smem = smem_sm / (C::SMEM + (int)fa.sharedSizeBytes + 1024);
     per_sm = max(1, min(min(by_regs, by_smem), min(8, 512 / (2 * C::NCOL))));
   }
   alignas(64) CUtensorMap mx;
