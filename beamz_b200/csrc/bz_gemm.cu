@@ -722,12 +722,15 @@ bool tc_eligible(const GemmP& p) {
 // descriptor (8-row atoms of 128-byte rows along K, atoms SBO = 1024 bytes apart, the
 // second 64-pixel block LBO = 128 K bytes after the first; a K step of 16 moves the
 // start address by two atoms). W^T is the K-major B operand, written once per CTA by
-// the threads in the no-swizzle core-matrix layout. A CTA of 128 threads walks tiles
-// (design b, 128 pixels) with a MIX_S-stage TMA ring: per tile, thread 0 issues K/16
-// MMAs into M TMEM columns and commits them; the four warps read their 32 pixels' rows
-// with tcgen05.ld and apply the epilogue (f32 term, biases, pre-activation, GELU), every
-// load and store coalesced along the pixels. Memory-bound (K = 32: 64 bytes read and
-// 64-192 bytes written per pixel), so several CTAs share an SM and their epilogues
+// the threads in the no-swizzle core-matrix layout. A persistent CTA of 128 threads
+// walks tiles (design b, 128 pixels) with a four-stage TMA ring and two TMEM
+// accumulators of M columns: while the four warps run tile j's epilogue, thread 0 has
+// already issued tile j+1's K/16 MMAs into the other accumulator. Each warp first loads
+// its 32 pixels' f32 term (independent of the MMAs), then waits for tile j's commit,
+// reads its rows with tcgen05.ld and applies the epilogue (f32 term, biases,
+// pre-activation, GELU), every load and store coalesced along the pixels. Memory-bound
+// (K = 32: 64 bytes read and 64-192 bytes written per pixel), so the grid is sized for
+// as many CTAs per SM as registers, shared memory and TMEM allow, and their epilogues
 // keep loads in flight. Bounded waits as in the GEMMs above.
 namespace mix {
 constexpr int S = 4, TP = 128, THREADS = 128;
