@@ -965,110 +965,194 @@ int launch_mix(const GemmP& p, cudaStream_t st) {
 }
 
 // ---- spectral channel mixing: O[b][o][k] = sum_c U[b][c][k] * W[k][c][o] (complex) ---
-// U, O: [B][C][n_modes][2] bf16 (re, im); W: [n_modes][Ci][Co][2] bf16. One block per
-// mode: the mode's weights and a chunk of SB designs' coefficients are staged in shared
-// memory (as float2), then every thread forms whole output sums from there.
-constexpr int SB = 64;     // designs per shared-memory chunk
+// U, O: [B][C][n_modes][2] bf16 (re, im); W: [n_modes][Ci][Co][2] bf16. A block takes KB
+// consecutive modes, so every global access moves KB complex values (16 bytes) per
+// channel row instead of one, and stages the modes' weights and a chunk of designs'
+// coefficients in shared memory as float2 (mode index fastest, so the lanes of a warp
+// read consecutive words). Each thread keeps several outputs in registers; when the
+// output index step 256 is a multiple of KB x channels (UNI: channels a power of two up
+// to 64), all of a thread's outputs share one weight (forward) or one coefficient row
+// (backward) per reduction step, which is then read once. Sums run in the same order
+// with the same fused multiply-adds for every block shape.
+constexpr int KB = 4;      // consecutive modes per block
+constexpr int DB = 16;     // designs per block (forward)
+constexpr int DBB = 8;     // designs per shared-memory chunk (backward)
 constexpr int SMAXC = 32;  // channels supported by the staged kernels
 
 __device__ __forceinline__ float2 ld_c(const bf16* p) {
   return make_float2(__bfloat162float(p[0]), __bfloat162float(p[1]));
 }
 
+__device__ __forceinline__ void st_c(bf16* p, float re, float im) {
+  *reinterpret_cast<__nv_bfloat162*>(p) = __floats2bfloat162_rn(re, im);
+}
+
+// grid (ceil(n_modes / KB), ceil(B / DB)), 256 threads
+template <bool UNI>
 __global__ void __launch_bounds__(256) spectral_fwd_kernel(const bf16* __restrict__ U, const bf16* __restrict__ W,
                                                            bf16* __restrict__ O, int B, int Ci, int Co, int nk) {
-  __shared__ float2 sw[SMAXC * SMAXC];
-  __shared__ float2 su[SB * SMAXC];
-  const int k = blockIdx.x;
-  for (int t = threadIdx.x; t < Ci * Co; t += blockDim.x) sw[t] = ld_c(W + ((long long)k * Ci * Co + t) * 2);
-  for (int b0 = 0; b0 < B; b0 += SB) {
-    const int nb = min(SB, B - b0);
-    __syncthreads();
-    for (int t = threadIdx.x; t < nb * Ci; t += blockDim.x) {
-      const int b = t / Ci, c = t - b * Ci;
-      su[t] = ld_c(U + (((long long)(b0 + b) * Ci + c) * nk + k) * 2);
+  __shared__ float2 sw[SMAXC * SMAXC * KB];  // [c][o][kk]
+  __shared__ float2 su[DB * SMAXC * KB];     // [b][c][kk]
+  constexpr int NJ = DB * SMAXC * KB / 256;  // outputs per thread
+  const int k0 = blockIdx.x * KB, b0 = blockIdx.y * DB;
+  const int nkb = min(KB, nk - k0), nb = min(DB, B - b0), CC = Ci * Co;
+  for (int t = threadIdx.x; t < KB * CC; t += 256) {  // along o: contiguous reads
+    const int kk = t / CC, r = t - kk * CC;
+    sw[r * KB + kk] = kk < nkb ? ld_c(W + ((long long)(k0 + kk) * CC + r) * 2) : make_float2(0.f, 0.f);
+  }
+  for (int t = threadIdx.x; t < nb * Ci * KB; t += 256) {  // KB consecutive modes per channel row
+    const int kk = t % KB, bc = t / KB;
+    su[t] = kk < nkb ? ld_c(U + (((long long)b0 * Ci + bc) * nk + k0 + kk) * 2) : make_float2(0.f, 0.f);
+  }
+  __syncthreads();
+  const int n_out = nb * Co * KB;
+  int ub[NJ], wo[NJ];
+  float re[NJ], im[NJ];
+#pragma unroll
+  for (int j = 0; j < NJ; ++j) {  // output i = (b, o, kk), kk fastest
+    const int i = threadIdx.x + 256 * j;
+    const int kk = i % KB, bo = i / KB, b = bo / Co, o = bo - b * Co;
+    const bool in = i < n_out;
+    ub[j] = in ? b * Ci * KB + kk : 0;
+    wo[j] = in ? o * KB + kk : 0;
+    re[j] = 0.f;
+    im[j] = 0.f;
+  }
+  for (int c = 0; c < Ci; ++c) {
+#pragma unroll
+    for (int j = 0; j < NJ; ++j) {
+      const float2 w = sw[c * Co * KB + (UNI ? wo[0] : wo[j])];
+      const float2 u = su[ub[j] + c * KB];
+      re[j] = fmaf(u.x, w.x, fmaf(-u.y, w.y, re[j]));
+      im[j] = fmaf(u.x, w.y, fmaf(u.y, w.x, im[j]));
     }
-    __syncthreads();
-    for (int t = threadIdx.x; t < nb * Co; t += blockDim.x) {
-      const int b = t / Co, o = t - b * Co;
-      float re = 0.f, im = 0.f;
-      for (int c = 0; c < Ci; ++c) {
-        const float2 u = su[b * Ci + c], w = sw[c * Co + o];
-        re = fmaf(u.x, w.x, fmaf(-u.y, w.y, re));
-        im = fmaf(u.x, w.y, fmaf(u.y, w.x, im));
-      }
-      bf16* q = O + (((long long)(b0 + b) * Co + o) * nk + k) * 2;
-      q[0] = __float2bfloat16_rn(re);
-      q[1] = __float2bfloat16_rn(im);
+  }
+#pragma unroll
+  for (int j = 0; j < NJ; ++j) {
+    const int i = threadIdx.x + 256 * j;
+    const int kk = i % KB, bo = i / KB;
+    if (i < n_out && kk < nkb) {
+      const int b = bo / Co, o = bo - b * Co;
+      st_c(O + (((long long)(b0 + b) * Co + o) * nk + k0 + kk) * 2, re[j], im[j]);
     }
   }
 }
 
-// Backward of one mode: dU[b][c] = sum_o dO[b][o] conj(W[c][o]); dW[c][o] += sum_b dO[b][o]
-// conj(U[b][c]) (f32).
+// Backward of KB modes: dU[b][c] = sum_o dO[b][o] conj(W[c][o]); dW[c][o] += sum_b dO[b][o]
+// conj(U[b][c]) (f32; one block owns its modes' dW, so no atomics). grid ceil(n_modes / KB).
+template <bool UNI>
 __global__ void __launch_bounds__(256) spectral_bwd_kernel(const bf16* __restrict__ dO, const bf16* __restrict__ U,
                                                            const bf16* __restrict__ W, bf16* __restrict__ dU,
                                                            float* __restrict__ dW, int B, int Ci, int Co, int nk) {
-  __shared__ float2 sw[SMAXC * SMAXC];
-  __shared__ float2 su[SB * SMAXC];
-  __shared__ float2 sg[SB * SMAXC];
-  const int k = blockIdx.x;
-  for (int t = threadIdx.x; t < Ci * Co; t += blockDim.x) sw[t] = ld_c(W + ((long long)k * Ci * Co + t) * 2);
-  // each thread owns (c, o) pairs t, t + blockDim, ... of dW
-  float2 acc[(SMAXC * SMAXC + 255) / 256];
+  __shared__ float2 sw[SMAXC * SMAXC * KB];  // [o][c][kk]
+  __shared__ float2 su[DBB * SMAXC * KB];    // [b][c][kk]
+  __shared__ float2 sg[DBB * SMAXC * KB];    // [b][o][kk]
+  constexpr int NW = SMAXC * SMAXC * KB / 256;  // dW outputs per thread
+  constexpr int NU = DBB * SMAXC * KB / 256;    // dU outputs per thread and chunk
+  const int k0 = blockIdx.x * KB, nkb = min(KB, nk - k0), CC = Ci * Co;
+  for (int t = threadIdx.x; t < KB * CC; t += 256) {
+    const int kk = t / CC, r = t - kk * CC, c = r / Co, o = r - c * Co;
+    sw[(o * Ci + c) * KB + kk] = kk < nkb ? ld_c(W + ((long long)(k0 + kk) * CC + r) * 2) : make_float2(0.f, 0.f);
+  }
+  // dW outputs i = (c, o, kk), kk fastest
+  const int n_w = CC * KB;
+  float ar[NW], ai[NW];
 #pragma unroll
-  for (int i = 0; i < (SMAXC * SMAXC + 255) / 256; ++i) acc[i] = make_float2(0.f, 0.f);
-  for (int b0 = 0; b0 < B; b0 += SB) {
-    const int nb = min(SB, B - b0);
+  for (int j = 0; j < NW; ++j) {
+    ar[j] = 0.f;
+    ai[j] = 0.f;
+  }
+  for (int bb = 0; bb < B; bb += DBB) {
+    const int nb = min(DBB, B - bb);
     __syncthreads();
-    for (int t = threadIdx.x; t < nb * Ci; t += blockDim.x) {
-      const int b = t / Ci, c = t - b * Ci;
-      su[t] = ld_c(U + (((long long)(b0 + b) * Ci + c) * nk + k) * 2);
+    for (int t = threadIdx.x; t < nb * Ci * KB; t += 256) {
+      const int kk = t % KB, bc = t / KB;
+      su[t] = kk < nkb ? ld_c(U + (((long long)bb * Ci + bc) * nk + k0 + kk) * 2) : make_float2(0.f, 0.f);
     }
-    for (int t = threadIdx.x; t < nb * Co; t += blockDim.x) {
-      const int b = t / Co, o = t - b * Co;
-      sg[t] = ld_c(dO + (((long long)(b0 + b) * Co + o) * nk + k) * 2);
+    for (int t = threadIdx.x; t < nb * Co * KB; t += 256) {
+      const int kk = t % KB, bo = t / KB;
+      sg[t] = kk < nkb ? ld_c(dO + (((long long)bb * Co + bo) * nk + k0 + kk) * 2) : make_float2(0.f, 0.f);
     }
     __syncthreads();
-    for (int t = threadIdx.x; t < nb * Ci; t += blockDim.x) {
-      const int b = t / Ci, c = t - b * Ci;
-      float re = 0.f, im = 0.f;
-      for (int o = 0; o < Co; ++o) {
-        const float2 g = sg[b * Co + o], w = sw[c * Co + o];
-        re = fmaf(g.x, w.x, fmaf(g.y, w.y, re));
-        im = fmaf(g.y, w.x, fmaf(-g.x, w.y, im));
+    // dU outputs i = (b, c, kk), kk fastest
+    const int n_u = nb * Ci * KB;
+    int gb[NU], wc[NU];
+    float ur[NU], ui[NU];
+#pragma unroll
+    for (int j = 0; j < NU; ++j) {
+      const int i = threadIdx.x + 256 * j;
+      const int kk = i % KB, bc = i / KB, b = bc / Ci, c = bc - b * Ci;
+      const bool in = i < n_u;
+      gb[j] = in ? b * Co * KB + kk : 0;
+      wc[j] = in ? c * KB + kk : 0;
+      ur[j] = 0.f;
+      ui[j] = 0.f;
+    }
+    for (int o = 0; o < Co; ++o) {
+#pragma unroll
+      for (int j = 0; j < NU; ++j) {
+        const float2 w = sw[o * Ci * KB + (UNI ? wc[0] : wc[j])];
+        const float2 g = sg[gb[j] + o * KB];
+        ur[j] = fmaf(g.x, w.x, fmaf(g.y, w.y, ur[j]));
+        ui[j] = fmaf(g.y, w.x, fmaf(-g.x, w.y, ui[j]));
       }
-      bf16* q = dU + (((long long)(b0 + b) * Ci + c) * nk + k) * 2;
-      q[0] = __float2bfloat16_rn(re);
-      q[1] = __float2bfloat16_rn(im);
     }
 #pragma unroll
-    for (int i = 0; i < (SMAXC * SMAXC + 255) / 256; ++i) {
-      const int t = threadIdx.x + i * 256;
-      if (t >= Ci * Co) break;
-      const int c = t / Co, o = t - c * Co;
-      float2 a = acc[i];
-      for (int b = 0; b < nb; ++b) {
-        const float2 g = sg[b * Co + o], u = su[b * Ci + c];
-        a.x = fmaf(g.x, u.x, fmaf(g.y, u.y, a.x));
-        a.y = fmaf(g.y, u.x, fmaf(-g.x, u.y, a.y));
+    for (int j = 0; j < NU; ++j) {
+      const int i = threadIdx.x + 256 * j;
+      const int kk = i % KB, bc = i / KB;
+      if (i < n_u && kk < nkb) st_c(dU + (((long long)bb * Ci + bc) * nk + k0 + kk) * 2, ur[j], ui[j]);
+    }
+    // dW: conj(U) dO summed over this chunk's designs, in design order
+    for (int b = 0; b < nb; ++b) {
+#pragma unroll
+      for (int j = 0; j < NW; ++j) {
+        const int i = threadIdx.x + 256 * j;
+        const int kk = i % KB, co = i / KB, c = co / Co, o = co - c * Co;
+        const bool in = i < n_w;
+        const float2 g = sg[b * Co * KB + (in ? o * KB + kk : 0)];
+        const float2 u = su[b * Ci * KB + (in ? c * KB + kk : 0)];
+        ar[j] = fmaf(g.x, u.x, fmaf(g.y, u.y, ar[j]));
+        ai[j] = fmaf(g.y, u.x, fmaf(-g.x, u.y, ai[j]));
       }
-      acc[i] = a;
     }
   }
 #pragma unroll
-  for (int i = 0; i < (SMAXC * SMAXC + 255) / 256; ++i) {
-    const int t = threadIdx.x + i * 256;
-    if (t >= Ci * Co) break;
-    float* d = dW + ((long long)k * Ci * Co + t) * 2;
-    d[0] += acc[i].x;
-    d[1] += acc[i].y;
+  for (int j = 0; j < NW; ++j) {
+    const int i = threadIdx.x + 256 * j;
+    const int kk = i % KB, co = i / KB;
+    if (i < n_w && kk < nkb) {
+      const int c = co / Co, o = co - c * Co;
+      float* d = dW + ((long long)(k0 + kk) * CC + c * Co + o) * 2;
+      d[0] += ar[j];
+      d[1] += ai[j];
+    }
   }
 }
 
+// dx = dy * GELU'(pre); VEC: 8 values per thread and step with 16-byte accesses (all three
+// arrays 16-byte aligned, n a multiple of 8).
+template <bool VEC>
 __global__ void gelu_bwd_kernel(const bf16* __restrict__ dy, const bf16* __restrict__ pre, bf16* __restrict__ dx,
                                 long long n) {
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  if (VEC) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n / 8; i += stride) {
+      const uint4 a = __ldg(reinterpret_cast<const uint4*>(dy) + i), q = __ldg(reinterpret_cast<const uint4*>(pre) + i);
+      const __nv_bfloat162* a2 = reinterpret_cast<const __nv_bfloat162*>(&a);
+      const __nv_bfloat162* q2 = reinterpret_cast<const __nv_bfloat162*>(&q);
+      uint4 r;
+      __nv_bfloat162* r2 = reinterpret_cast<__nv_bfloat162*>(&r);
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        const float2 av = __bfloat1622float2(a2[e]), qv = __bfloat1622float2(q2[e]);
+        r2[e] = __floats2bfloat162_rn(av.x * gelu_grad(qv.x), av.y * gelu_grad(qv.y));
+      }
+      reinterpret_cast<uint4*>(dx)[i] = r;
+    }
+    return;
+  }
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += stride)
     dx[i] = __float2bfloat16_rn(__bfloat162float(dy[i]) * gelu_grad(__bfloat162float(pre[i])));
 }
 
@@ -1085,12 +1169,26 @@ __global__ void row_mean_kernel(const bf16* __restrict__ x, float* __restrict__ 
 }
 
 // Sum over rows: out[c] += sum_b sum_p x[b][c][p] (bf16 in, f32 out); one block per
-// (c, b) row of P values, reduced in the block and added atomically.
+// (c, b) row of P values, reduced in the block and added atomically. VEC: rows 16-byte
+// aligned (P a multiple of 8), read 8 values per thread and step.
+template <bool VEC>
 __global__ void chan_sum_kernel(const bf16* __restrict__ x, float* __restrict__ out, int B, int C, int P) {
   const int c = blockIdx.x, b = blockIdx.y;
   const bf16* row = x + ((long long)b * C + c) * P;
   float s = 0.f;
-  for (int p = threadIdx.x; p < P; p += blockDim.x) s += __bfloat162float(row[p]);
+  if (VEC) {
+    for (int p = threadIdx.x; p < P / 8; p += blockDim.x) {
+      const uint4 a = __ldg(reinterpret_cast<const uint4*>(row) + p);
+      const __nv_bfloat162* a2 = reinterpret_cast<const __nv_bfloat162*>(&a);
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        const float2 v = __bfloat1622float2(a2[e]);
+        s += v.x + v.y;
+      }
+    }
+  } else {
+    for (int p = threadIdx.x; p < P; p += blockDim.x) s += __bfloat162float(row[p]);
+  }
   __shared__ float red[32];
   for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
   if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
@@ -1102,11 +1200,26 @@ __global__ void chan_sum_kernel(const bf16* __restrict__ x, float* __restrict__ 
   }
 }
 
-// x[r][p] = g[r] * scale (broadcast of a per-row gradient), bf16 out.
+// x[r][p] = g[r] * scale (broadcast of a per-row gradient), bf16 out; VEC: P a multiple of
+// 8 and x 16-byte aligned, 8 values per thread and step.
+template <bool VEC>
 __global__ void row_broadcast_kernel(const float* __restrict__ g, bf16* __restrict__ x, long long rows, int P,
                                      float scale) {
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  if (VEC) {
+    const int P8 = P / 8;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < rows * P8; i += stride) {
+      const __nv_bfloat162 v = __float2bfloat162_rn(__ldg(g + i / P8) * scale);
+      uint4 r;
+      __nv_bfloat162* r2 = reinterpret_cast<__nv_bfloat162*>(&r);
+#pragma unroll
+      for (int e = 0; e < 4; ++e) r2[e] = v;
+      reinterpret_cast<uint4*>(x)[i] = r;
+    }
+    return;
+  }
   const long long n = rows * P;
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += stride)
     x[i] = __float2bfloat16_rn(g[i / P] * scale);
 }
 
@@ -1227,8 +1340,14 @@ extern "C" int bz_spectral_mix(const void* U, const void* W, void* O, int32_t B,
   BZ_REQUIRE(U && W && O, "bz_spectral_mix: NULL buffer");
   BZ_REQUIRE(B >= 1 && ci >= 1 && co >= 1 && ci <= bz::SMAXC && co <= bz::SMAXC && n_modes >= 1,
              "bz_spectral_mix: bad sizes (channels up to %d)", bz::SMAXC);
-  bz::spectral_fwd_kernel<<<(unsigned)n_modes, 256, 0, bz::as_stream(stream)>>>(
-      (const bz::bf16*)U, (const bz::bf16*)W, (bz::bf16*)O, B, ci, co, n_modes);
+  BZ_REQUIRE(B <= 65535 * bz::DB, "bz_spectral_mix: batch above %d", 65535 * bz::DB);
+  const dim3 grid((unsigned)bz::ceil_div(n_modes, bz::KB), (unsigned)bz::ceil_div(B, bz::DB));
+  if (256 % (bz::KB * co) == 0)
+    bz::spectral_fwd_kernel<true><<<grid, 256, 0, bz::as_stream(stream)>>>((const bz::bf16*)U, (const bz::bf16*)W,
+                                                                          (bz::bf16*)O, B, ci, co, n_modes);
+  else
+    bz::spectral_fwd_kernel<false><<<grid, 256, 0, bz::as_stream(stream)>>>((const bz::bf16*)U, (const bz::bf16*)W,
+                                                                           (bz::bf16*)O, B, ci, co, n_modes);
   return bz::check_launch("bz_spectral_mix");
 }
 
@@ -1237,16 +1356,26 @@ extern "C" int bz_spectral_mix_bwd(const void* dO, const void* U, const void* W,
   BZ_REQUIRE(dO && U && W && dU && dW, "bz_spectral_mix_bwd: NULL buffer");
   BZ_REQUIRE(B >= 1 && ci >= 1 && co >= 1 && ci <= bz::SMAXC && co <= bz::SMAXC && n_modes >= 1,
              "bz_spectral_mix_bwd: bad sizes (channels up to %d)", bz::SMAXC);
-  bz::spectral_bwd_kernel<<<(unsigned)n_modes, 256, 0, bz::as_stream(stream)>>>(
-      (const bz::bf16*)dO, (const bz::bf16*)U, (const bz::bf16*)W, (bz::bf16*)dU, dW, B, ci, co, n_modes);
+  const unsigned grid = (unsigned)bz::ceil_div(n_modes, bz::KB);
+  if (256 % (bz::KB * ci) == 0)
+    bz::spectral_bwd_kernel<true><<<grid, 256, 0, bz::as_stream(stream)>>>(
+        (const bz::bf16*)dO, (const bz::bf16*)U, (const bz::bf16*)W, (bz::bf16*)dU, dW, B, ci, co, n_modes);
+  else
+    bz::spectral_bwd_kernel<false><<<grid, 256, 0, bz::as_stream(stream)>>>(
+        (const bz::bf16*)dO, (const bz::bf16*)U, (const bz::bf16*)W, (bz::bf16*)dU, dW, B, ci, co, n_modes);
   return bz::check_launch("bz_spectral_mix_bwd");
 }
 
 extern "C" int bz_gelu_bwd(const void* dy, const void* pre, void* dx, int64_t n, void* stream) {
   BZ_REQUIRE(dy && pre && dx && n >= 0, "bz_gelu_bwd: bad arguments");
   if (n == 0) return BZ_OK;
-  bz::gelu_bwd_kernel<<<bz::grid_for(n, 256), 256, 0, bz::as_stream(stream)>>>(
-      (const bz::bf16*)dy, (const bz::bf16*)pre, (bz::bf16*)dx, n);
+  auto al = [](const void* q) { return (reinterpret_cast<uintptr_t>(q) & 15u) == 0u; };
+  if (n % 8 == 0 && al(dy) && al(pre) && al(dx))
+    bz::gelu_bwd_kernel<true><<<bz::grid_for(n / 8, 256), 256, 0, bz::as_stream(stream)>>>(
+        (const bz::bf16*)dy, (const bz::bf16*)pre, (bz::bf16*)dx, n);
+  else
+    bz::gelu_bwd_kernel<false><<<bz::grid_for(n, 256), 256, 0, bz::as_stream(stream)>>>(
+        (const bz::bf16*)dy, (const bz::bf16*)pre, (bz::bf16*)dx, n);
   return bz::check_launch("bz_gelu_bwd");
 }
 
@@ -1261,16 +1390,24 @@ extern "C" int bz_row_mean(const void* x, float* out, int64_t rows, int32_t P, f
 extern "C" int bz_row_broadcast(const float* g, void* x, int64_t rows, int32_t P, float scale, void* stream) {
   BZ_REQUIRE(g && x && rows >= 0 && P >= 1, "bz_row_broadcast: bad arguments");
   if (rows == 0) return BZ_OK;
-  bz::row_broadcast_kernel<<<bz::grid_for(rows * P, 256), 256, 0, bz::as_stream(stream)>>>(g, (bz::bf16*)x, rows, P,
-                                                                                          scale);
+  if (P % 8 == 0 && (reinterpret_cast<uintptr_t>(x) & 15u) == 0u)
+    bz::row_broadcast_kernel<true><<<bz::grid_for(rows * (P / 8), 256), 256, 0, bz::as_stream(stream)>>>(
+        g, (bz::bf16*)x, rows, P, scale);
+  else
+    bz::row_broadcast_kernel<false><<<bz::grid_for(rows * P, 256), 256, 0, bz::as_stream(stream)>>>(
+        g, (bz::bf16*)x, rows, P, scale);
   return bz::check_launch("bz_row_broadcast");
 }
 
 extern "C" int bz_chan_sum(const void* x, float* out, int32_t B, int32_t C, int32_t P, void* stream) {
   BZ_REQUIRE(x && out && B >= 1 && C >= 1 && P >= 1, "bz_chan_sum: bad arguments");
   BZ_REQUIRE(B <= 65535, "bz_chan_sum: B above 65535");
-  bz::chan_sum_kernel<<<dim3((unsigned)C, (unsigned)B), 256, 0, bz::as_stream(stream)>>>((const bz::bf16*)x, out, B,
-                                                                                        C, P);
+  if (P % 8 == 0 && (reinterpret_cast<uintptr_t>(x) & 15u) == 0u)
+    bz::chan_sum_kernel<true><<<dim3((unsigned)C, (unsigned)B), 256, 0, bz::as_stream(stream)>>>(
+        (const bz::bf16*)x, out, B, C, P);
+  else
+    bz::chan_sum_kernel<false><<<dim3((unsigned)C, (unsigned)B), 256, 0, bz::as_stream(stream)>>>(
+        (const bz::bf16*)x, out, B, C, P);
   return bz::check_launch("bz_chan_sum");
 }
 

@@ -231,6 +231,67 @@ def test_tcgen05_channel_mixing_matches_mma_sync_and_f32(bz, K, M, ta, N):
     assert rel(outf, res[1][0]) <= 1e-5
 
 
+@pytest.mark.parametrize("B,ci,co,nk", [(64, 32, 32, 512), (5, 8, 8, 30), (19, 12, 20, 37)])
+def test_spectral_mixing_kernels_match_complex_products(bz, B, ci, co, nk):
+    """bz_spectral_mix / bz_spectral_mix_bwd against complex float64 products of the same
+    bf16 values: O = sum_c U W, dU = sum_o dO conj(W), dW += sum_b dO conj(U). Shapes
+    cover mode counts that leave a partial group of four modes, batches that leave a
+    partial chunk, and channel counts that are not powers of two."""
+    from beamz_b200 import _native as nat
+
+    g = torch.Generator().manual_seed(B * 100 + ci + co + nk)
+    U = torch.randn(B, ci, nk, 2, generator=g).to(torch.bfloat16)
+    W = (torch.randn(nk, ci, co, 2, generator=g) / ci ** 0.5).to(torch.bfloat16)
+    dO = torch.randn(B, co, nk, 2, generator=g).to(torch.bfloat16)
+    dW0 = torch.randn(nk, ci, co, 2, generator=g)
+    cU = torch.view_as_complex(U.double().contiguous())
+    cW = torch.view_as_complex(W.double().contiguous())
+    cG = torch.view_as_complex(dO.double().contiguous())
+    want_O = torch.einsum("bck,kco->bok", cU, cW)
+    want_dU = torch.einsum("bok,kco->bck", cG, cW.conj())
+    want_dW = dW0.double() + torch.view_as_real(torch.einsum("bok,bck->kco", cG, cU.conj()))
+    dev = "cuda"
+    Ud, Wd, dOd = U.to(dev), W.to(dev), dO.to(dev)
+    O = torch.empty(B, co, nk, 2, dtype=torch.bfloat16, device=dev)
+    dU = torch.empty(B, ci, nk, 2, dtype=torch.bfloat16, device=dev)
+    dW = dW0.to(dev)
+    st = torch.cuda.current_stream().cuda_stream
+    nat.spectral_mix(Ud.data_ptr(), Wd.data_ptr(), O.data_ptr(), B, ci, co, nk, st)
+    nat.spectral_mix_bwd(dOd.data_ptr(), Ud.data_ptr(), Wd.data_ptr(), dU.data_ptr(), dW.data_ptr(), B, ci, co, nk,
+                         st)
+    torch.cuda.synchronize()
+    assert rel(O.double(), torch.view_as_real(want_O)) <= 8e-3
+    assert rel(dU.double(), torch.view_as_real(want_dU)) <= 8e-3
+    assert rel(dW, want_dW) <= 1e-5
+
+
+@pytest.mark.parametrize("B,C,P", [(4, 8, 576), (3, 5, 37)])
+def test_elementwise_surrogate_kernels(bz, B, C, P):
+    """GELU backward, per-channel sums and the per-row broadcast against torch on the same
+    bf16 values; P = 576 takes the 16-byte paths, P = 37 the scalar ones."""
+    from beamz_b200 import _native as nat
+
+    g = torch.Generator().manual_seed(B + C + P)
+    dy = torch.randn(B, C, P, generator=g).to(torch.bfloat16)
+    pre = torch.randn(B, C, P, generator=g).to(torch.bfloat16)
+    rows = torch.randn(B * C, generator=g)
+    pre64 = pre.double().requires_grad_(True)
+    fno_ref.gelu(pre64).backward(dy.double())
+    dev, st = "cuda", torch.cuda.current_stream().cuda_stream
+    dyd, pred = dy.to(dev), pre.to(dev)
+    dx = torch.empty_like(dyd)
+    nat.gelu_bwd(dyd.data_ptr(), pred.data_ptr(), dx.data_ptr(), dx.numel(), st)
+    sums = torch.full((C,), 0.5, device=dev)
+    nat.chan_sum(dyd.data_ptr(), sums.data_ptr(), B, C, P, st)
+    bc = torch.empty(B * C, P, dtype=torch.bfloat16, device=dev)
+    rows_d = rows.to(dev)
+    nat.row_broadcast(rows_d.data_ptr(), bc.data_ptr(), B * C, P, 0.25, st)
+    torch.cuda.synchronize()
+    assert rel(dx.float(), pre64.grad) <= 8e-3
+    assert rel(sums, 0.5 + dy.double().sum(dim=(0, 2))) <= 1e-5
+    assert torch.equal(bc.cpu(), (rows * 0.25).to(torch.bfloat16)[:, None].expand(B * C, P))
+
+
 def test_fno_with_tcgen05_spectral_gemms_matches_oracle(bz):
     """n = 64, 8 modes, width 32, batch 8: the DFT GEMMs (M = 256, N = 256, K = 4096)
     and their inverses run on the tcgen05 kernel."""
