@@ -964,6 +964,161 @@ int launch_mix(const GemmP& p, cudaStream_t st) {
   return p.M == 32 ? launch_mix_kc_mc<64, 32>(p, st) : launch_mix_kc_mc<64, 64>(p, st);
 }
 
+// ---- tcgen05 weight gradients: outf[M][N] += alpha sum_b A[b] (M x K) B[b]^T (K x N) -----
+// The surrogate's 1x1-layer weight gradients: both operands are activations with the K
+// pixels contiguous (K-major), M (<= 128) and N (16..128) channel rows, summed over the
+// pixels and the batch. A persistent CTA takes a contiguous range of (design, 64-pixel)
+// items, loads each item's M + N rows by TMA (128-byte swizzle) through a four-stage ring
+// and accumulates all of them into one TMEM tile with 128 x N x 16 MMAs (rows M..127 of
+// the A stage are never loaded: their accumulator rows are not read); at the end the
+// warps holding rows below M add alpha times their rows to outf atomically. Memory-bound:
+// (M + N) x 2 bytes per pixel and design.
+namespace wg {
+constexpr int S = 4, BK = 64, THREADS = 128, A_ST = 128 * BK * 2;
+}
+
+template <int NC>
+__global__ void __launch_bounds__(wg::THREADS) wgrad_tc_kernel(const __grid_constant__ CUtensorMap tmA,
+                                                              const __grid_constant__ CUtensorMap tmB, GemmP p,
+                                                              int n_items, int items_b) {
+  constexpr int B_ST = NC * wg::BK * 2, STAGE = wg::A_ST + B_ST, NCOL = NC < 32 ? 32 : NC;
+  constexpr uint32_t IDESC = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(NC >> 3) << 17) | (8u << 24);
+  extern __shared__ unsigned char smem_raw[];
+  unsigned char* smem = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  unsigned char* bar = smem + wg::S * STAGE;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bar + 8 * (2 * wg::S + 1));
+  const uint32_t sbase = static_cast<uint32_t>(__cvta_generic_to_shared(smem));
+  const uint32_t full0 = static_cast<uint32_t>(__cvta_generic_to_shared(bar));
+  const uint32_t empty0 = full0 + 8 * wg::S, done = full0 + 16 * wg::S;
+  const uint32_t tx = (uint32_t)(p.M + NC) * wg::BK * 2;
+  // this CTA's items [i0, i1): item i = (design i / items_b, pixels 64 (i % items_b) ...)
+  const int per = (n_items + (int)gridDim.x - 1) / (int)gridDim.x;
+  const int i0 = min(n_items, (int)blockIdx.x * per), i1 = min(n_items, i0 + per), nt = i1 - i0;
+
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(
+                     static_cast<uint32_t>(__cvta_generic_to_shared(tmem_slot))),
+                 "r"(NCOL));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::);
+  }
+  if (tid == 0) {
+    for (int i = 0; i < 2 * wg::S + 1; ++i) asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(full0 + 8 * i));
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;\n" ::);
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
+  const uint32_t taddr = *tmem_slot;
+
+  int ok = 1;
+  if (tid == 0 && nt > 0) {
+    auto issue = [&](int t) {  // item i0 + t into stage t % S
+      const int i = i0 + t, b = i / items_b, k0 = (i - b * items_b) * wg::BK;
+      const uint32_t st = sbase + (t % wg::S) * STAGE, fb = full0 + 8 * (t % wg::S);
+      asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(fb), "r"(tx) : "memory");
+      tma_load_2d(st, &tmA, k0, b * p.M, fb);
+      tma_load_2d(st + wg::A_ST, &tmB, k0, b * NC, fb);
+    };
+    int issued = 0, consumed = 0;
+    for (; issued < min(wg::S, nt); ++issued) issue(issued);
+    for (int it = 0; it < nt; ++it) {
+      const int s = it % wg::S;
+      if (!tc_wait(full0 + 8 * s, (uint32_t)((it / wg::S) & 1), p.wait_limit)) {
+        ok = 0;
+        break;
+      }
+      consumed = it + 1;
+      asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
+      const uint32_t a0 = sbase + s * STAGE, b0 = a0 + wg::A_ST;
+#pragma unroll
+      for (int kk = 0; kk < wg::BK / 16; ++kk) {
+        const uint64_t da = tc_sdesc_sw128(a0 + kk * 32);
+        const uint64_t db = tc_sdesc_sw128(b0 + kk * 32);
+        asm volatile(
+            "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+            "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n"
+            :
+            : "r"(taddr), "l"(da), "l"(db), "r"(IDESC), "r"((it > 0 || kk > 0) ? 1u : 0u), "r"(0u), "r"(0u),
+              "r"(0u), "r"(0u));
+      }
+      asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(
+          empty0 + 8 * s));
+      if (it >= 1 && issued < nt) {  // refill the previous stage once its MMAs are done
+        const int sp = (it - 1) % wg::S;
+        if (!tc_wait(empty0 + 8 * sp, (uint32_t)(((it - 1) / wg::S) & 1), p.wait_limit)) {
+          ok = 0;
+          break;
+        }
+        issue(issued++);
+      }
+    }
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(done));
+    for (int t = consumed; t < issued; ++t)  // copies still in flight after a failure
+      tc_wait(full0 + 8 * (t % wg::S), (uint32_t)((t / wg::S) & 1), p.wait_limit);
+  }
+  ok = __syncthreads_and(ok);
+  if (nt > 0 && !tc_wait(done, 0u, p.wait_limit)) ok = 0;
+  ok = __syncthreads_and(ok);
+  if (!ok && tid == 0) atomicExch(&g_tc_error, 1);
+  asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
+  if (ok && nt > 0 && warp * 32 < p.M) {  // warps holding accumulator rows below M
+    const int m = warp * 32 + lane;
+#pragma unroll
+    for (int c0 = 0; c0 < NC; c0 += 32) {
+      uint32_t v[32];
+      tmem_ld32(taddr + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, v);
+      if (m < p.M) {
+#pragma unroll
+        for (int e = 0; e < 32 && c0 + e < NC; ++e) atomicAdd(p.outf + (long long)m * p.ldc + c0 + e, p.alpha * __uint_as_float(v[e]));
+      }
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;\n" ::);
+  __syncthreads();
+  if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(taddr), "r"(NCOL));
+}
+
+// The weight-gradient kernel takes: ta = 0, tb = 1, atomic with sc = 0 (a sum over the
+// batch; any split-K request is met by its own split over items), M <= 128, N = 32 or 64,
+// K >= 64, rows 16-byte aligned with the designs back to back (sa = M lda, sb = N ldb).
+bool wgrad_eligible(const GemmP& p) {
+  auto al = [](const void* q) { return (reinterpret_cast<uintptr_t>(q) & 15u) == 0u; };
+  return !p.ta && p.tb && p.atomic && p.sc == 0 && p.outf && p.M >= 1 && p.M <= 128 && (p.N == 32 || p.N == 64) &&
+         p.K >= 64 && p.lda % 8 == 0 && p.ldb % 8 == 0 && p.sa == (long long)p.M * p.lda &&
+         p.sb == (long long)p.N * p.ldb && al(p.A) && al(p.B) && (long long)p.batch * 128 <= (1LL << 31) - 1;
+}
+
+template <int NC>
+int launch_wgrad_nc(const GemmP& p, cudaStream_t st) {
+  constexpr int SMEM = wg::S * (wg::A_ST + NC * wg::BK * 2) + 8 * (2 * wg::S + 1) + 16 + 1024;
+  static bool configured = false;
+  if (!configured) {
+    if (cudaFuncSetAttribute(wgrad_tc_kernel<NC>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM) != cudaSuccess)
+      return fail(BZ_ERR_CUDA, "bz_gemm_bf16: cannot configure the weight-gradient kernel's shared memory");
+    configured = true;
+  }
+  alignas(64) CUtensorMap ma, mb;
+  if (!make_map(&ma, p.A, (long long)p.batch * p.M, p.K, p.lda, p.M) ||
+      !make_map(&mb, p.B, (long long)p.batch * NC, p.K, p.ldb, NC))
+    return 0;
+  int dev = 0, sms = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const int items_b = (int)ceil_div(p.K, wg::BK);
+  const long long n_items = (long long)p.batch * items_b;
+  if (n_items > (1LL << 31) - 1) return 0;
+  const int grid = (int)(n_items < 2LL * sms ? n_items : 2LL * sms);  // two CTAs per SM (80-96 KB each)
+  wgrad_tc_kernel<NC><<<grid, wg::THREADS, SMEM, st>>>(ma, mb, p, (int)n_items, items_b);
+  const int rc = check_launch("bz_gemm_bf16");
+  return rc == BZ_OK ? 1 : rc;
+}
+
+// 1: launched; 0: not applicable; <0: error status.
+int launch_wgrad(const GemmP& p, cudaStream_t st) {
+  return p.N == 32 ? launch_wgrad_nc<32>(p, st) : launch_wgrad_nc<64>(p, st);
+}
+
 // ---- spectral channel mixing: O[b][o][k] = sum_c U[b][c][k] * W[k][c][o] (complex) ---
 // U, O: [B][C][n_modes][2] bf16 (re, im); W: [n_modes][Ci][Co][2] bf16. A block takes KB
 // consecutive modes, so every global access moves KB complex values (16 bytes) per
@@ -1282,6 +1437,10 @@ extern "C" int bz_gemm_bf16(const bz_gemm* g, void* stream) {
     const int t = bz::launch_gemm_tma(p, st);
     if (t != 0) return t > 0 ? BZ_OK : t;
     return bz::launch_gemm_tc(p, st);
+  }
+  if (g->engine == 0 && bz::wgrad_eligible(p)) {
+    const int t = bz::launch_wgrad(p, st);
+    if (t != 0) return t > 0 ? BZ_OK : t;
   }
   if (g->engine == 0 && bz::mix_eligible(p)) {
     const int t = bz::launch_mix(p, st);

@@ -422,7 +422,9 @@ typedef struct bz_gemm {
                                    the GEMM kernel for ta = 0, tb = 1, M >= 128, N >= 256,
                                    K >= 64, 16-byte aligned rows (TMA-fed when batch = 1); the
                                    channel-mixing kernel for tb = 0, K and M in {32, 64},
-                                   N >= 64, sb = K * ldb, no atomic / split-K;
+                                   N >= 64, sb = K * ldb, no atomic / split-K; the
+                                   weight-gradient kernel for ta = 0, tb = 1, atomic, sc = 0,
+                                   M <= 128, N in {32, 64}, sa = M * lda, sb = N * ldb;
                                    1: mma.sync only;
                                    2: the register-staged tcgen05 kernel where eligible */
   const void* A;

@@ -292,6 +292,41 @@ def test_elementwise_surrogate_kernels(bz, B, C, P):
     assert torch.equal(bc.cpu(), (rows * 0.25).to(torch.bfloat16)[:, None].expand(B * C, P))
 
 
+@pytest.mark.parametrize("M,N,K", [(32, 32, 14400), (64, 32, 1000), (32, 64, 4096)])
+def test_tcgen05_weight_gradient_matches_mma_sync_and_f32(bz, M, N, K):
+    """The tcgen05 weight-gradient kernel (engine 0: outf += sum_b A[b] B[b]^T with both
+    operands pixel-contiguous) against the mma.sync kernel (engine 1, split-K 3) and an
+    f32 sum of the same bf16 values, accumulating onto a nonzero output; K = 1000 leaves
+    a partial 64-pixel item."""
+    from beamz_b200 import _native as nat
+
+    g = torch.Generator().manual_seed(M + N + K)
+    batch = 5
+    A = torch.randn(batch, M, K, generator=g).to(torch.bfloat16)
+    Bm = torch.randn(batch, N, K, generator=g).to(torch.bfloat16)
+    init = torch.randn(M, N, generator=g)
+    want = init.double() + 0.5 * torch.einsum("bmk,bnk->mn", A.double(), Bm.double())
+    dev = "cuda"
+    Ad, Bd = A.to(dev), Bm.to(dev)
+    outs = {}
+    nat.gemm_error(reset=True)
+    for engine in (0, 1):
+        out = init.to(dev)
+        p = nat.Gemm()
+        p.M, p.N, p.K, p.batch, p.splitk, p.act, p.ta, p.tb, p.atomic = M, N, K, batch, 3, 0, 0, 1, 1
+        p.engine = engine
+        p.A, p.lda, p.sa = Ad.data_ptr(), K, M * K
+        p.B, p.ldb, p.sb = Bd.data_ptr(), K, N * K
+        p.alpha = 0.5
+        p.outf, p.ldc, p.sc = out.data_ptr(), N, 0
+        nat.gemm(p, torch.cuda.current_stream().cuda_stream)
+        torch.cuda.synchronize()
+        outs[engine] = out
+    assert nat.gemm_error(reset=True) == 0
+    assert rel(outs[0], want) <= 1e-5
+    assert rel(outs[0], outs[1]) <= 1e-5
+
+
 def test_fno_with_tcgen05_spectral_gemms_matches_oracle(bz):
     """n = 64, 8 modes, width 32, batch 8: the DFT GEMMs (M = 256, N = 256, K = 4096)
     and their inverses run on the tcgen05 kernel."""
