@@ -68,7 +68,7 @@ class Gemm(C.Structure):
                 ("tb", i32), ("atomic", i32), ("engine", i32), ("A", vp), ("lda", i64), ("sa", i64), ("B", vp),
                 ("ldb", i64), ("sb", i64), ("alpha", C.c_float), ("reserved2", C.c_float), ("cadd", vp),
                 ("ldadd", i64), ("sadd", i64), ("bias_m", vp), ("bias_n", vp), ("outf", vp), ("outh", vp),
-                ("ldc", i64), ("sc", i64), ("pre", vp), ("ldpre", i64), ("spre", i64)]
+                ("ldc", i64), ("sc", i64), ("pre", vp), ("ldpre", i64), ("spre", i64), ("cadd_h", vp)]
 
 
 class Grid3D(C.Structure):

@@ -45,6 +45,7 @@ struct GemmP {
   long long ldc, sc;
   bf16* pre;
   long long ldpre, spre;
+  const bf16* cadd_h;  // the added term in bf16 instead of f32 (same strides), or null
   int wait_limit;  // polls of a bounded mbarrier wait before it gives up (tcgen05 kernel)
   int withhold;    // 1: the tcgen05 kernel issues no MMA for its first K slice (timeout self-test)
 };
@@ -244,6 +245,9 @@ __global__ void __launch_bounds__(32 * WM * WN) gemm_bf16_kernel(GemmP p) {
           } else {
             for (int e = 0; e < cnt; ++e) v[e] += q[e];
           }
+        } else if (p.cadd_h) {
+          const bf16* q = p.cadd_h + (long long)bz * p.sadd + (long long)m * p.ldadd + n;
+          for (int e = 0; e < cnt; ++e) v[e] += __bfloat162float(q[e]);
         }
         for (int e = 0; e < cnt; ++e) {
           if (p.bias_m) v[e] += p.bias_m[m];
@@ -457,6 +461,7 @@ __global__ void __launch_bounds__(tc::THREADS) gemm_tc_kernel(GemmP p) {
         if (m >= p.M || n >= p.N) continue;
         float x = p.alpha * __uint_as_float(v[e]);
         if (p.cadd) x += p.cadd[(long long)bz * p.sadd + (long long)m * p.ldadd + n];
+        else if (p.cadd_h) x += __bfloat162float(p.cadd_h[(long long)bz * p.sadd + (long long)m * p.ldadd + n]);
         if (p.bias_m) x += p.bias_m[m];
         if (p.bias_n) x += p.bias_n[n];
         if (p.pre) p.pre[(long long)bz * p.spre + (long long)m * p.ldpre + n] = __float2bfloat16_rn(x);
@@ -612,8 +617,11 @@ __global__ void __launch_bounds__(tc::THREADS) gemm_tma_kernel(const __grid_cons
   asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
   const int m = m0 + warp * 32 + lane;
   // plain f32 output (no epilogue terms): two 16-byte stores per 8 columns
-  const bool plain = p.outf && !p.atomic && !p.outh && !p.cadd && !p.bias_m && !p.bias_n && !p.pre && p.act == 0 &&
+  const bool plain = p.outf && !p.atomic && !p.outh && !p.cadd && !p.cadd_h && !p.bias_m && !p.bias_n && !p.pre && p.act == 0 &&
                      (p.ldc & 3) == 0 && ((reinterpret_cast<uintptr_t>(p.outf) & 15u) == 0u);
+  // plain bf16 output: one 16-byte store per 8 columns
+  const bool plain_h = p.outh && !p.outf && !p.atomic && !p.cadd && !p.cadd_h && !p.bias_m && !p.bias_n && !p.pre &&
+                       p.act == 0 && (p.ldc & 7) == 0 && ((reinterpret_cast<uintptr_t>(p.outh) & 15u) == 0u);
   if (ok) {
     for (int c0 = 0; c0 < tc::BN; c0 += 8) {
       uint32_t v[8];
@@ -633,6 +641,13 @@ __global__ void __launch_bounds__(tc::THREADS) gemm_tma_kernel(const __grid_cons
                            p.alpha * __uint_as_float(v[2]), p.alpha * __uint_as_float(v[3]));
         q[1] = make_float4(p.alpha * __uint_as_float(v[4]), p.alpha * __uint_as_float(v[5]),
                            p.alpha * __uint_as_float(v[6]), p.alpha * __uint_as_float(v[7]));
+      } else if (plain_h && m < p.M && n0 + c0 + 8 <= p.N) {
+        uint4 w;
+        __nv_bfloat162* h = reinterpret_cast<__nv_bfloat162*>(&w);
+#pragma unroll
+        for (int e = 0; e < 4; ++e)
+          h[e] = __floats2bfloat162_rn(p.alpha * __uint_as_float(v[2 * e]), p.alpha * __uint_as_float(v[2 * e + 1]));
+        *reinterpret_cast<uint4*>(p.outh + (long long)m * p.ldc + n0 + c0) = w;
       } else {
 #pragma unroll
         for (int e = 0; e < 8; ++e) {
@@ -640,6 +655,7 @@ __global__ void __launch_bounds__(tc::THREADS) gemm_tma_kernel(const __grid_cons
           if (m >= p.M || n >= p.N) continue;
           float x = p.alpha * __uint_as_float(v[e]);
           if (p.cadd) x += p.cadd[(long long)m * p.ldadd + n];
+          else if (p.cadd_h) x += __bfloat162float(p.cadd_h[(long long)m * p.ldadd + n]);
           if (p.bias_m) x += p.bias_m[m];
           if (p.bias_n) x += p.bias_n[n];
           if (p.pre) p.pre[(long long)m * p.ldpre + n] = __float2bfloat16_rn(x);
@@ -856,6 +872,10 @@ __global__ void __launch_bounds__(mix::THREADS) mix_tc_kernel(const __grid_const
       const float* q = p.cadd + (long long)b * p.sadd + n;
 #pragma unroll
       for (int e = 0; e < MC; ++e) add[e] = __ldg(q + (long long)e * p.ldadd);
+    } else if (p.cadd_h && live) {
+      const bf16* q = p.cadd_h + (long long)b * p.sadd + n;
+#pragma unroll
+      for (int e = 0; e < MC; ++e) add[e] = __bfloat162float(q[(long long)e * p.ldadd]);
     }
     if (tid == 0 && j + 1 < n_my) {  // next tile into the other accumulator (read out by iteration j - 1)
       if (mma(j + 1)) mmas = j + 2; else ok = 0;
@@ -1413,7 +1433,8 @@ extern "C" int bz_gemm_bf16(const bz_gemm* g, void* stream) {
              "bz_gemm_bf16: bad sizes M=%d N=%d K=%d batch=%d splitk=%d", g->M, g->N, g->K, g->batch, g->splitk);
   BZ_REQUIRE(g->A && g->B, "bz_gemm_bf16: NULL operand");
   BZ_REQUIRE(g->outf || g->outh, "bz_gemm_bf16: no output");
-  BZ_REQUIRE(!(g->atomic || g->splitk > 1) || (g->outf && !g->outh && !g->cadd && !g->bias_m && !g->bias_n &&
+  BZ_REQUIRE(!(g->cadd && g->cadd_h), "bz_gemm_bf16: give the added term as f32 or as bf16, not both");
+  BZ_REQUIRE(!(g->atomic || g->splitk > 1) || (g->outf && !g->outh && !g->cadd && !g->cadd_h && !g->bias_m && !g->bias_n &&
                                                 !g->pre && g->act == 0),
              "bz_gemm_bf16: atomic/split-K output takes a plain f32 product only");
   BZ_REQUIRE(g->splitk == 1 || g->atomic, "bz_gemm_bf16: split-K needs atomic accumulation");
@@ -1427,6 +1448,7 @@ extern "C" int bz_gemm_bf16(const bz_gemm* g, void* stream) {
   p.B = (const bz::bf16*)g->B; p.ldb = g->ldb; p.sb = g->sb;
   p.alpha = g->alpha;
   p.cadd = g->cadd; p.ldadd = g->ldadd; p.sadd = g->sadd;
+  p.cadd_h = (const bz::bf16*)g->cadd_h;
   p.bias_m = g->bias_m; p.bias_n = g->bias_n;
   p.outf = g->outf; p.outh = (bz::bf16*)g->outh; p.ldc = g->ldc; p.sc = g->sc;
   p.pre = (bz::bf16*)g->pre; p.ldpre = g->ldpre; p.spre = g->spre;

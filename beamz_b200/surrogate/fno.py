@@ -101,14 +101,14 @@ class FNO2d:
         return torch.cuda.current_stream().cuda_stream
 
     def _gemm(self, M, N, K, A, lda, B, ldb, *, batch=1, sa=0, sb=0, ta=0, tb=0, outf=None, outh=None, ldc=None,
-              sc=0, cadd=None, ldadd=0, sadd=0, bias_m=None, bias_n=None, act=0, pre=None, atomic=0, splitk=1,
-              alpha=1.0):
+              sc=0, cadd=None, cadd_h=None, ldadd=0, sadd=0, bias_m=None, bias_n=None, act=0, pre=None, atomic=0,
+              splitk=1, alpha=1.0):
         g = nat.Gemm()
         g.M, g.N, g.K, g.batch, g.splitk, g.act = M, N, K, batch, splitk, act
         g.ta, g.tb, g.atomic = ta, tb, atomic
         g.A, g.lda, g.sa, g.B, g.ldb, g.sb = _p(A), lda, sa, _p(B), ldb, sb
         g.alpha = alpha
-        g.cadd, g.ldadd, g.sadd = _p(cadd), ldadd, sadd
+        g.cadd, g.cadd_h, g.ldadd, g.sadd = _p(cadd), _p(cadd_h), ldadd, sadd
         g.bias_m, g.bias_n = _p(bias_m), _p(bias_n)
         g.outf, g.outh = _p(outf), _p(outh)
         g.ldc, g.sc = (N if ldc is None else ldc), sc
@@ -162,12 +162,13 @@ class FNO2d:
             U = self._dft(V, B)
             O = torch.empty_like(U)
             nat.spectral_mix(U.data_ptr(), p[f"R{l}"].h.data_ptr(), O.data_ptr(), B, C, C, self.K, self._stream())
-            S = torch.empty((B * C, P), dtype=torch.float32, device=self.dev)
-            self._gemm(B * C, P, 2 * self.K, O, 2 * self.K, self.GT, 2 * self.K, tb=1, outf=S)
+            # the spectral branch in bf16 (half the bytes of the write and of its read-back)
+            S = torch.empty((B * C, P), dtype=BF16, device=self.dev)
+            self._gemm(B * C, P, 2 * self.K, O, 2 * self.K, self.GT, 2 * self.K, tb=1, outh=S)
             act = 1 if l < self.L else 0
             pre = torch.empty((B, C, P), dtype=BF16, device=self.dev) if act else None
             Vn = torch.empty((B, C, P), dtype=BF16, device=self.dev)
-            self._gemm(C, P, C, p[f"W{l}"].h, C, V, P, batch=B, sb=C * P, outh=Vn, sc=C * P, cadd=S, ldadd=P,
+            self._gemm(C, P, C, p[f"W{l}"].h, C, V, P, batch=B, sb=C * P, outh=Vn, sc=C * P, cadd_h=S, ldadd=P,
                        sadd=C * P, bias_m=p[f"b{l}"].w, act=act, pre=pre)
             del S
             acts["U"].append(U)
@@ -229,10 +230,10 @@ class FNO2d:
             dU = torch.empty_like(dOm)
             nat.spectral_mix_bwd(dOm.data_ptr(), a["U"][l - 1].data_ptr(), p[f"R{l}"].h.data_ptr(), dU.data_ptr(),
                                  p[f"R{l}"].g.data_ptr(), B, C, C, self.K, st)
-            dVs = torch.empty((B * C, P), dtype=torch.float32, device=self.dev)
-            self._gemm(B * C, P, 2 * self.K, dU, 2 * self.K, self.F, 2 * self.K, tb=1, outf=dVs)
+            dVs = torch.empty((B * C, P), dtype=BF16, device=self.dev)
+            self._gemm(B * C, P, 2 * self.K, dU, 2 * self.K, self.F, 2 * self.K, tb=1, outh=dVs)
             dVn = torch.empty((B, C, P), dtype=BF16, device=self.dev)
-            self._gemm(C, P, C, p[f"W{l}"].h, C, dV, P, ta=1, batch=B, sb=C * P, outh=dVn, sc=C * P, cadd=dVs,
+            self._gemm(C, P, C, p[f"W{l}"].h, C, dV, P, ta=1, batch=B, sb=C * P, outh=dVn, sc=C * P, cadd_h=dVs,
                        ldadd=P, sadd=C * P)
             dV = dVn
         nat.chan_sum(dV.data_ptr(), p["b0"].g.data_ptr(), B, C, P, st)

@@ -410,7 +410,7 @@ int bz_rasterize3d(int32_t nx, int32_t ny, int32_t nz, int32_t n_zs, const doubl
  * op(A)[m][k] = A[m*lda + k] (ta = 0) or A[k*lda + m] (ta = 1); op(B)[k][n] =
  * B[k*ldb + n] (tb = 0) or B[n*ldb + k] (tb = 1); sa/sb/sc/sadd/spre are batch
  * strides in elements (0 shares an operand across the batch). Epilogue, in order:
- * + cadd[b][m][n] (f32, optional), + bias_m[m], + bias_n[n] (f32, optional), a copy
+ * + cadd[b][m][n] (f32, or bf16 as cadd_h; optional), + bias_m[m], + bias_n[n] (f32, optional), a copy
  * to pre (bf16, optional), act (0 none, 1 GELU tanh form), then store to outf (f32)
  * and/or outh (bf16). atomic = 1 adds alpha*product into outf (f32 only, no other
  * epilogue term), which with sc = 0 reduces over the batch; splitk > 1 splits K
@@ -441,6 +441,7 @@ typedef struct bz_gemm {
   int64_t ldc, sc;
   void* pre;
   int64_t ldpre, spre;
+  const void* cadd_h;           /* the added term as bf16 instead of cadd (same ldadd/sadd) */
 } bz_gemm;
 
 int bz_gemm_bf16(const bz_gemm* g, void* stream);

@@ -327,6 +327,61 @@ def test_tcgen05_weight_gradient_matches_mma_sync_and_f32(bz, M, N, K):
     assert rel(outs[0], outs[1]) <= 1e-5
 
 
+@pytest.mark.parametrize("K,M,N", [(32, 32, 14400), (32, 64, 200)])
+def test_channel_mixing_with_bf16_term(bz, K, M, N):
+    """The mixing kernel and the mma.sync kernel with the added term given in bf16
+    (cadd_h), as the surrogate passes its spectral branch: against f32 of the same values."""
+    from beamz_b200 import _native as nat
+
+    g = torch.Generator().manual_seed(K + M + N)
+    batch = 3
+    W = torch.randn(M, K, generator=g).to(torch.bfloat16)
+    X = torch.randn(batch, K, N, generator=g).to(torch.bfloat16)
+    add = torch.randn(batch, M, N, generator=g).to(torch.bfloat16)
+    want = torch.einsum("mk,bkn->bmn", W.float(), X.float()) + add.float()
+    dev = "cuda"
+    Wd, Xd, addd = W.to(dev), X.to(dev), add.to(dev)
+    for engine in (0, 1):
+        outh = torch.empty(batch, M, N, device=dev, dtype=torch.bfloat16)
+        p = nat.Gemm()
+        p.M, p.N, p.K, p.batch, p.splitk, p.act, p.ta, p.tb, p.atomic = M, N, K, batch, 1, 0, 0, 0, 0
+        p.engine = engine
+        p.A, p.lda, p.sa = Wd.data_ptr(), K, 0
+        p.B, p.ldb, p.sb = Xd.data_ptr(), N, K * N
+        p.alpha = 1.0
+        p.cadd_h, p.ldadd, p.sadd = addd.data_ptr(), N, M * N
+        p.outh, p.ldc, p.sc = outh.data_ptr(), N, M * N
+        nat.gemm(p, torch.cuda.current_stream().cuda_stream)
+        torch.cuda.synchronize()
+        assert rel(outh.float(), want) <= 8e-3, engine
+
+
+def test_tma_gemm_plain_bf16_output(bz):
+    """The TMA-fed tcgen05 GEMM storing bf16 only (16-byte stores per 8 columns, the
+    surrogate's inverse transform): against f32 of the same bf16 operands, with a partial
+    last column tile."""
+    from beamz_b200 import _native as nat
+
+    M, N, K = 256, 600, 192
+    g = torch.Generator().manual_seed(11)
+    A = torch.randn(M, K, generator=g).to(torch.bfloat16)
+    Bt = torch.randn(N, K, generator=g).to(torch.bfloat16)
+    want = A.float() @ Bt.float().t()
+    dev = "cuda"
+    Ad, Bd = A.to(dev), Bt.to(dev)
+    outh = torch.empty(M, N, device=dev, dtype=torch.bfloat16)
+    p = nat.Gemm()
+    p.M, p.N, p.K, p.batch, p.splitk, p.act, p.ta, p.tb, p.atomic, p.engine = M, N, K, 1, 1, 0, 0, 1, 0, 0
+    p.A, p.lda, p.B, p.ldb = Ad.data_ptr(), K, Bd.data_ptr(), K
+    p.alpha = 1.0
+    p.outh, p.ldc = outh.data_ptr(), N
+    nat.gemm_error(reset=True)
+    nat.gemm(p, torch.cuda.current_stream().cuda_stream)
+    torch.cuda.synchronize()
+    assert nat.gemm_error(reset=True) == 0
+    assert rel(outh.float(), want) <= 8e-3
+
+
 def test_fno_with_tcgen05_spectral_gemms_matches_oracle(bz):
     """n = 64, 8 modes, width 32, batch 8: the DFT GEMMs (M = 256, N = 256, K = 4096)
     and their inverses run on the tcgen05 kernel."""
