@@ -8,12 +8,14 @@
 // are staged through registers into padded shared memory with the reduction dim
 // (K) contiguous whatever the operands' layouts (80-byte rows keep ldmatrix free
 // of bank conflicts), double buffered, and multiplied by warps with
-// mma.sync.m16n8k16 (bf16 inputs, f32 accumulators). The epilogue adds an f32
-// term, row/column biases, applies GELU, and stores f32 and/or bf16, or
+// mma.sync.m16n8k16 (bf16 inputs, f32 accumulators). The epilogue adds an f32 (or
+// bf16) term, row/column biases, applies GELU, and stores f32 and/or bf16, or
 // accumulates atomically (batch-reduced or split-K weight gradients). Where the
 // shapes allow, bz_gemm_bf16 runs tcgen05/TMEM kernels instead: the large DFT GEMMs
-// (TMA-fed, 128 x 256 tiles) and the 1x1 channel mixing (pixel-contiguous
-// activations as an MN-major TMA operand); both are described below.
+// (TMA-fed, 128 x 256 tiles), the 1x1 channel mixing (pixel-contiguous activations
+// as an MN-major TMA operand) and its weight gradients (both operands K-major,
+// reduced over pixels and designs); each is described below. The mma.sync kernel
+// remains for the shapes they do not take (the 3-channel lift layer, the pooled head).
 #include <cuda.h>
 #include <cuda_bf16.h>
 
